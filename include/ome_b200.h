@@ -1,0 +1,169 @@
+/*
+ * ome_b200.h -- C ABI of libomeb200.so, a B200 (sm_100a) einsum engine that
+ * plugs in behind OMEinsum.jl's backend registry.
+ *
+ * Plain C: pointers, sizes and int status codes.  No exceptions cross this
+ * boundary and the library never aborts the process.  Every compute entry
+ * point takes an explicit CUDA stream (passed as void*, i.e. a cudaStream_t)
+ * and is asynchronous on it.
+ *
+ * Conventions (those of OMEinsum.jl):
+ *   - tensors are strided views; dims[d] is the extent of dimension d and
+ *     strides[d] its step in ELEMENTS (NULL strides = column-major contiguous,
+ *     Julia's layout: dimension 1 fastest);
+ *   - labels are int32 (Julia Char code points or Int labels);
+ *   - y <- sy*y + sx*f(xs); sx, sy point to one value of the call's dtype;
+ *     sy equal to the algebra's zero means "overwrite" (y is not read), as in
+ *     the iszero(sy) branch of @addmul! (src/utils.jl:25-35);
+ *   - all inputs and the output share one dtype (the caller converts mixed
+ *     eltypes first, like CUDAExt.jl:116 / align_eltypes, src/utils.jl:108-115);
+ *   - the output must not alias an input.
+ */
+#ifndef OME_B200_H
+#define OME_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define OME_API __attribute__((visibility("default")))
+#else
+#define OME_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes.  Mapping to Julia exceptions on the Julia side:
+ * INVALID_ARGUMENT -> ArgumentError, DIMENSION_MISMATCH -> DimensionMismatch
+ * (src/interfaces.jl:78-88,100), everything else -> ErrorException. */
+typedef enum {
+  OME_OK = 0,
+  OME_INVALID_ARGUMENT = 1,
+  OME_DIMENSION_MISMATCH = 2,
+  OME_UNSUPPORTED = 3,
+  OME_OUT_OF_MEMORY = 4,
+  OME_TIMEOUT = 5,      /* a bounded device-side wait gave up */
+  OME_CUDA_ERROR = 6
+} ome_status;
+
+/* Element types.  BOOL is one byte per element, contracted as OR-AND.
+ * TROP_F32/TROP_F64 are TropicalNumbers.jl Tropical{Float32/Float64}:
+ * (+) = max, (*) = +, zero = -Inf, one = 0.  Complex types are interleaved
+ * (re, im) pairs, Julia's ComplexF32/ComplexF64. */
+typedef enum {
+  OME_F32 = 0,
+  OME_F64 = 1,
+  OME_C32 = 2,
+  OME_C64 = 3,
+  OME_I64 = 4,
+  OME_BOOL = 5,
+  OME_TROP_F32 = 6,
+  OME_TROP_F64 = 7
+} ome_dtype;
+
+/* Precision mode for F32/C32 contractions.
+ * OME_PREC_AUTO   : BF16x3 split products on the tensor cores where the
+ *                   contraction is GEMM-shaped, exact-type CUDA-core code elsewhere.
+ * OME_PREC_FP32   : CUDA-core FP32 FMA everywhere (the plain GPU path).
+ * OME_PREC_BF16X3 : same as AUTO.
+ * Other dtypes ignore it. */
+typedef enum { OME_PREC_AUTO = 0, OME_PREC_FP32 = 1, OME_PREC_BF16X3 = 2 } ome_prec;
+
+typedef struct {
+  void* data;
+  int32_t ndim;
+  const int64_t* dims;
+  const int64_t* strides; /* elements; NULL = column-major contiguous */
+  const int32_t* labels;  /* ndim labels */
+} ome_tensor;
+
+typedef struct ome_ctx ome_ctx;
+typedef struct ome_plan ome_plan;
+
+/* Library / context ------------------------------------------------------- */
+
+/* ABI version of this header. */
+OME_API int ome_version(void);
+
+/* Number of kernels this library has launched since it was loaded (all
+ * threads); lets a caller count device launches in a timed region. */
+OME_API unsigned long long ome_launch_count(void);
+
+/* Message of the last failed call on this host thread ("" if none). */
+OME_API const char* ome_last_error(void);
+
+/* Create a context on `device` with a device workspace of `workspace_bytes`
+ * (intermediates of plans and scratch of single calls).  Replaces the per-
+ * intermediate CUDA.jl allocations (ext/CUDAExt.jl:34-47, :129-131). */
+OME_API int ome_ctx_create(int device, size_t workspace_bytes, ome_ctx** out);
+OME_API int ome_ctx_destroy(ome_ctx* ctx);
+OME_API int ome_ctx_workspace_bytes(const ome_ctx* ctx, size_t* out);
+
+/* Single contractions ------------------------------------------------------ */
+
+/* einsum!(ixs, iy, xs, y, sx, sy, size_dict) for any number of inputs.
+ * Replaces: the backend dispatch override ext/CUDAExt.jl:181-192 (binary),
+ * the unary einsum! src/einsum.jl:84-101 with its rules src/unaryrules.jl,
+ * and the n-ary fallback src/einsum.jl:47-50 -> loop_einsum!.
+ * Dispatch: 1 input -> fused unary kernels; 2 inputs -> strided GEMM (no
+ * permuted copies) or the index kernel; >= 3 inputs -> the index kernel. */
+OME_API int ome_einsum(ome_ctx* ctx, void* stream, ome_dtype dtype, int32_t ninputs,
+               const ome_tensor* xs, const ome_tensor* y, const void* sx,
+               const void* sy, int32_t prec);
+
+/* loop_einsum!(ixs, iy, xs, y, sx, sy, size_dict): the generic index-iterating
+ * kernel regardless of shape.  Replaces src/loop_einsum.jl:21-45 and its GPU
+ * form ext/CUDAExt.jl:60-113 (mapreducedim! over EinArray + expanddims!). */
+OME_API int ome_loop_einsum(ome_ctx* ctx, void* stream, ome_dtype dtype, int32_t ninputs,
+                    const ome_tensor* xs, const ome_tensor* y, const void* sx,
+                    const void* sy);
+
+/* Contraction trees (NestedEinsum / SlicedEinsum) -------------------------- */
+
+/* A tree is given in post-order, root last.  Node j has node_nargs[j]
+ * children; its child references are the next node_nargs[j] entries of
+ * node_args: r >= 0 is node r, r < 0 is input tensor (-r - 1).  Its output
+ * labels are the next node_niy[j] entries of node_iy.  The labels of input
+ * tensor t are the next input_nlabels[t] entries of input_labels.  Extents:
+ * label_ids[i] has extent label_extents[i].  Sliced labels (SlicedEinsum,
+ * src/slicing.jl:10-13) are iterated in column-major order (first fastest).
+ * Replaces einsum!/einsum(::NestedEinsum) (src/einsequence.jl:270-287,
+ * ext/CUDAExt.jl:121-147) and the SlicedEinsum executors
+ * (src/slicing.jl:112-137). */
+OME_API int ome_plan_create(ome_ctx* ctx, ome_dtype dtype, int32_t ninputs,
+                    const int32_t* input_nlabels, const int32_t* input_labels,
+                    int32_t nnodes, const int32_t* node_nargs,
+                    const int32_t* node_args, const int32_t* node_niy,
+                    const int32_t* node_iy, int32_t nlabels,
+                    const int32_t* label_ids, const int64_t* label_extents,
+                    int32_t nsliced, const int32_t* sliced_labels, int32_t prec,
+                    ome_plan** out);
+OME_API int ome_plan_destroy(ome_plan* plan);
+
+/* Peak workspace bytes the plan needs (forward only / forward+gradient). */
+OME_API int ome_plan_peak_bytes(const ome_plan* plan, size_t* forward_bytes, size_t* grad_bytes);
+
+/* Evaluate the tree: y <- sy*y + sx*tree(inputs).  inputs[t] are column-major
+ * contiguous device buffers; y is column-major contiguous.  With slices, the
+ * cross-slice sum is accumulated in FP64 for F32/F64 (C64 for C32). */
+OME_API int ome_plan_execute(ome_ctx* ctx, ome_plan* plan, void* stream,
+                     const void* const* inputs, void* y, const void* sx,
+                     const void* sy);
+
+/* cost_and_gradient (src/bp.jl:122-130): forward with every intermediate kept
+ * in the workspace, then einsum_grad (src/autodiff.jl:24-30) per node.
+ * dy: the output cotangent (NULL = ones, requires a scalar output).  y
+ * receives the forward value, dxs[t] the gradient of input t (column-major,
+ * same shape as the input).  Slicing is not used for gradients, as in the
+ * reference (src/bp.jl:26-28). */
+OME_API int ome_plan_gradient(ome_ctx* ctx, ome_plan* plan, void* stream,
+                      const void* const* inputs, const void* dy, void* y,
+                      void* const* dxs);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* OME_B200_H */

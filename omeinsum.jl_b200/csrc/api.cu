@@ -1,0 +1,604 @@
+// C ABI entry points and the single-contraction dispatcher of libomeb200.
+//
+// einsum! semantics follow OMEinsum.jl: unary (src/einsum.jl:84-101 with the
+// rules of src/unaryrules.jl), binary (src/einsum.jl:104-211 +
+// src/binaryrules.jl) and n-ary (src/einsum.jl:47-50 -> loop_einsum!).  The
+// B200 design differs from the reference's in how, not what:
+//  * repeated input labels (Diag) become diagonal views (summed strides) --
+//    no compactify! copy;
+//  * labels only on the output (Repeat) become stride-0 input modes;
+//  * repeated output labels (Duplicate) become a diagonal view of y after a
+//    one-pass y <- sy*y (or zero) over the off-diagonal entries;
+//  * binary contractions run as a strided GEMM whose mode strides absorb
+//    simplifyto's permutations (src/einsum.jl:127-134) and the output
+//    permutation, so no permuted temporary is written to HBM; dangling
+//    labels (summed on one side only) are pre-reduced as the reference does.
+#include <stdarg.h>
+#include <stdio.h>
+#include <string.h>
+#include <algorithm>
+#include <string>
+#include <vector>
+
+#include "dispatch.h"
+
+namespace ome {
+
+static thread_local std::string g_err;
+
+int set_err(int code, const char* fmt, ...) {
+  char buf[1024];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  g_err = buf;
+  return code;
+}
+
+int cuda_err(cudaError_t e, const char* what) {
+  if (e == cudaSuccess) return OME_OK;
+  if (e == cudaErrorMemoryAllocation) return set_err(OME_OUT_OF_MEMORY, "%s: %s", what, cudaGetErrorString(e));
+  return set_err(OME_CUDA_ERROR, "%s: %s", what, cudaGetErrorString(e));
+}
+
+#define OME_CK(call)                                   \
+  do {                                                 \
+    int rc_ = (call);                                  \
+    if (rc_ != OME_OK) return rc_;                     \
+  } while (0)
+#define OME_CUDA(call, what)                           \
+  do {                                                 \
+    cudaError_t e_ = (call);                           \
+    if (e_ != cudaSuccess) return cuda_err(e_, what);  \
+  } while (0)
+
+void* ws_alloc(ome_ctx* c, size_t bytes) {
+  size_t off = (c->ws_top + 255) & ~(size_t)255;
+  if (off + bytes > c->ws_bytes) return nullptr;
+  c->ws_top = off + bytes;
+  return c->ws + off;
+}
+
+// ----------------------------------------------------------------------------
+// scalars
+// ----------------------------------------------------------------------------
+
+Scalar scalar_from(ome_dtype dt, const void* p) {
+  Scalar s;
+  memset(&s, 0, sizeof(s));
+  memcpy(s.b, p, dtype_size(dt));
+  return s;
+}
+bool scalar_is_zero(ome_dtype dt, const Scalar& v) {
+  bool r = false;
+  OME_DISPATCH(dt, ALG, r = ALG::is_zero(scalar_as<typename ALG::T>(v)));
+  return r;
+}
+bool scalar_is_one(ome_dtype dt, const Scalar& v) {
+  bool r = false;
+  OME_DISPATCH(dt, ALG, r = ALG::is_one(scalar_as<typename ALG::T>(v)));
+  return r;
+}
+Scalar scalar_one(ome_dtype dt) {
+  Scalar s;
+  memset(&s, 0, sizeof(s));
+  OME_DISPATCH(dt, ALG, { typename ALG::T v = ALG::one(); memcpy(s.b, &v, sizeof(v)); });
+  return s;
+}
+Scalar scalar_zero(ome_dtype dt) {
+  Scalar s;
+  memset(&s, 0, sizeof(s));
+  OME_DISPATCH(dt, ALG, { typename ALG::T v = ALG::zero(); memcpy(s.b, &v, sizeof(v)); });
+  return s;
+}
+
+// ----------------------------------------------------------------------------
+// views
+// ----------------------------------------------------------------------------
+
+int view_from_tensor(const ome_tensor& t, HView& v, const char* what) {
+  if (t.ndim < 0 || t.ndim > MAXD)
+    return set_err(OME_INVALID_ARGUMENT, "%s: rank %d outside [0, %d]", what, t.ndim, MAXD);
+  if (t.ndim > 0 && (!t.dims || !t.labels))
+    return set_err(OME_INVALID_ARGUMENT, "%s: dims and labels are required", what);
+  v.data = static_cast<char*>(t.data);
+  v.nd = t.ndim;
+  int64_t s = 1;
+  for (int d = 0; d < t.ndim; ++d) {
+    if (t.dims[d] < 0) return set_err(OME_INVALID_ARGUMENT, "%s: negative extent", what);
+    v.ext[d] = t.dims[d];
+    v.str[d] = t.strides ? t.strides[d] : s;
+    v.lab[d] = t.labels[d];
+    s *= t.dims[d];
+  }
+  return OME_OK;
+}
+
+int unique_view(const HView& v, HView& u) {
+  u.data = v.data;
+  u.nd = 0;
+  for (int d = 0; d < v.nd; ++d) {
+    int k = 0;
+    for (; k < u.nd; ++k)
+      if (u.lab[k] == v.lab[d]) break;
+    if (k < u.nd) {
+      if (u.ext[k] != v.ext[d])
+        return set_err(OME_DIMENSION_MISMATCH, "label %d = %lld or %lld)?", v.lab[d],
+                       (long long)u.ext[k], (long long)v.ext[d]);
+      u.str[k] += v.str[d];
+    } else {
+      u.lab[u.nd] = v.lab[d];
+      u.ext[u.nd] = v.ext[d];
+      u.str[u.nd] = v.str[d];
+      u.nd++;
+    }
+  }
+  return OME_OK;
+}
+
+static int find_lab(const HView& v, int32_t l) {
+  for (int d = 0; d < v.nd; ++d)
+    if (v.lab[d] == l) return d;
+  return -1;
+}
+
+static int64_t numel(const HView& v) {
+  int64_t n = 1;
+  for (int d = 0; d < v.nd; ++d) n *= v.ext[d];
+  return n;
+}
+
+// ----------------------------------------------------------------------------
+// mode tables: one row per label, one stride column per tensor
+// ----------------------------------------------------------------------------
+
+struct Modes {
+  int n = 0, nt = 0;
+  int64_t ext[2 * MAXD];
+  int64_t str[MAXIN + 1][2 * MAXD];
+
+  void add(int64_t e, const int64_t* s) {
+    ext[n] = e;
+    for (int t = 0; t < nt; ++t) str[t][n] = s[t];
+    n++;
+  }
+  int64_t total() const {
+    int64_t p = 1;
+    for (int i = 0; i < n; ++i) p *= ext[i];
+    return p;
+  }
+  // Drop unit modes; stable sort by |stride of tensor key| (zero strides last);
+  // merge neighbours whose strides are consistent in every tensor.
+  void normalize(int key) {
+    int w = 0;
+    for (int i = 0; i < n; ++i) {
+      if (ext[i] == 1) continue;
+      ext[w] = ext[i];
+      for (int t = 0; t < nt; ++t) str[t][w] = str[t][i];
+      w++;
+    }
+    n = w;
+    std::vector<int> idx(n);
+    for (int i = 0; i < n; ++i) idx[i] = i;
+    auto k = [&](int i) -> uint64_t {
+      int64_t s = str[key][i];
+      if (s == 0) return ~0ull;
+      return (uint64_t)(s < 0 ? -s : s);
+    };
+    std::stable_sort(idx.begin(), idx.end(), [&](int a, int b) { return k(a) < k(b); });
+    int64_t e2[2 * MAXD], s2[MAXIN + 1][2 * MAXD];
+    for (int i = 0; i < n; ++i) {
+      e2[i] = ext[idx[i]];
+      for (int t = 0; t < nt; ++t) s2[t][i] = str[t][idx[i]];
+    }
+    int m = 0;
+    for (int i = 0; i < n; ++i) {
+      if (m > 0) {
+        bool ok = true;
+        for (int t = 0; t < nt && ok; ++t) ok = s2[t][i] == str[t][m - 1] * ext[m - 1];
+        if (ok) {
+          ext[m - 1] *= e2[i];
+          continue;
+        }
+      }
+      ext[m] = e2[i];
+      for (int t = 0; t < nt; ++t) str[t][m] = s2[t][i];
+      m++;
+    }
+    n = m;
+  }
+};
+
+// ----------------------------------------------------------------------------
+// generic index kernel
+// ----------------------------------------------------------------------------
+
+static int run_loop(ome_ctx* ctx, cudaStream_t s, ome_dtype dt, int nin, const HView* xu,
+                    const HView& yu, const Scalar& sx, const Scalar& sy, bool sy_zero) {
+  if (nin < 1 || nin > MAXIN)
+    return set_err(OME_UNSUPPORTED, "the index kernel takes 1..%d inputs, got %d", MAXIN, nin);
+  Modes outer, inner;
+  outer.nt = inner.nt = nin + 1;
+  int64_t st[MAXIN + 1];
+  for (int d = 0; d < yu.nd; ++d) {
+    st[0] = yu.str[d];
+    for (int i = 0; i < nin; ++i) {
+      int k = find_lab(xu[i], yu.lab[d]);
+      st[1 + i] = k >= 0 ? xu[i].str[k] : 0;
+    }
+    outer.add(yu.ext[d], st);
+  }
+  std::vector<int32_t> seen;
+  for (int i = 0; i < nin; ++i)
+    for (int d = 0; d < xu[i].nd; ++d) {
+      const int32_t l = xu[i].lab[d];
+      if (find_lab(yu, l) >= 0 || std::find(seen.begin(), seen.end(), l) != seen.end()) continue;
+      if ((int)seen.size() >= 2 * MAXD)
+        return set_err(OME_UNSUPPORTED, "index kernel: more than %d summed labels", 2 * MAXD);
+      seen.push_back(l);
+      st[0] = 0;
+      for (int j = 0; j < nin; ++j) {
+        int k = find_lab(xu[j], l);
+        st[1 + j] = k >= 0 ? xu[j].str[k] : 0;
+      }
+      inner.add(xu[i].ext[d], st);
+    }
+  const int64_t n_out = outer.total(), n_in = inner.total();
+  if (n_out == 0) return OME_OK;
+  outer.normalize(0);
+  inner.normalize(1);
+  if (outer.n + inner.n > MAXM)
+    return set_err(OME_UNSUPPORTED, "index kernel: %d modes after merging exceed %d", outer.n + inner.n, MAXM);
+
+  LoopArgs a;
+  memset(&a, 0, sizeof(a));
+  for (int i = 0; i < nin; ++i) a.x[i] = xu[i].data;
+  a.y = yu.data;
+  a.nin = nin;
+  a.nout = outer.n;
+  a.ninner = inner.n;
+  a.n_out = n_out;
+  a.n_in = n_in;
+  for (int m = 0; m < outer.n; ++m) {
+    a.ext[m] = outer.ext[m];
+    for (int t = 0; t <= nin; ++t) a.str[t][m] = outer.str[t][m];
+  }
+  for (int m = 0; m < inner.n; ++m) {
+    a.ext[outer.n + m] = inner.ext[m];
+    for (int t = 0; t <= nin; ++t) a.str[t][outer.n + m] = inner.str[t][m];
+  }
+  a.sx = sx;
+  a.sy = sy;
+  a.sy_zero = sy_zero;
+  a.sx_one = scalar_is_one(dt, sx);
+  a.nsplit = 1;
+
+  const int sms = ctx->num_sms;
+  const bool thread_mode = n_in <= 16 || n_out >= (int64_t)sms * 512;
+  if (thread_mode) {
+    const int64_t nb = (n_out + 255) / 256;
+    const int grid = (int)std::min<int64_t>(nb, (int64_t)sms * 16);
+    return cuda_err(launch_loop(dt, a, LOOP_THREAD, grid, 256, s), "index kernel");
+  }
+  const int block = 256;
+  int64_t nsplit = 1;
+  const int64_t target = (int64_t)sms * 8;
+  if (n_out < target) {
+    nsplit = (target + n_out - 1) / n_out;
+    nsplit = std::min<int64_t>(nsplit, std::max<int64_t>(1, n_in / (block * 8)));
+  }
+  if (nsplit > 1) {
+    a.partial = ws_alloc(ctx, (size_t)(n_out * nsplit) * dtype_size(dt));
+    if (!a.partial) nsplit = 1;
+  }
+  a.nsplit = (int)nsplit;
+  // step = block * nsplit in the inner mixed radix (last digit unbounded)
+  int64_t step = (int64_t)block * nsplit;
+  for (int m = 0; m < inner.n; ++m) {
+    if (m == inner.n - 1) {
+      a.stepdig[m] = (int32_t)std::min<int64_t>(step, 0x7fffffff);
+    } else {
+      a.stepdig[m] = (int32_t)(step % inner.ext[m]);
+      step /= inner.ext[m];
+    }
+  }
+  const int64_t nblocks = n_out * nsplit;
+  const int grid = (int)std::min<int64_t>(nblocks, (int64_t)sms * 32);
+  OME_CK(cuda_err(launch_loop(dt, a, LOOP_BLOCK, grid, block, s), "index kernel"));
+  if (nsplit > 1) OME_CK(cuda_err(launch_loop_finish(dt, a, s), "index kernel finish"));
+  return OME_OK;
+}
+
+// ----------------------------------------------------------------------------
+// unary: permute / broadcast copy, or reduction
+// ----------------------------------------------------------------------------
+
+static int run_unary(ome_ctx* ctx, cudaStream_t s, ome_dtype dt, const HView& xu, const HView& yu,
+                     const Scalar& sx, const Scalar& sy, bool sy_zero) {
+  bool reduced = false;
+  for (int d = 0; d < xu.nd; ++d)
+    if (find_lab(yu, xu.lab[d]) < 0 && xu.ext[d] != 1) reduced = true;
+  if (reduced || xu.nd == 0 && false) return run_loop(ctx, s, dt, 1, &xu, yu, sx, sy, sy_zero);
+  // labels of x not in y have extent 1 here (or 0, then y gets sy*y + sx*zero)
+  for (int d = 0; d < xu.nd; ++d)
+    if (find_lab(yu, xu.lab[d]) < 0 && xu.ext[d] == 0) return run_loop(ctx, s, dt, 1, &xu, yu, sx, sy, sy_zero);
+  Modes md;
+  md.nt = 2;  // 0: y, 1: x
+  int64_t st[2];
+  for (int d = 0; d < yu.nd; ++d) {
+    int k = find_lab(xu, yu.lab[d]);
+    st[0] = yu.str[d];
+    st[1] = k >= 0 ? xu.str[k] : 0;
+    md.add(yu.ext[d], st);
+  }
+  const int64_t n = md.total();
+  if (n == 0) return OME_OK;
+  md.normalize(0);
+  if (md.n > MAXM) return run_loop(ctx, s, dt, 1, &xu, yu, sx, sy, sy_zero);
+  PermArgs a;
+  memset(&a, 0, sizeof(a));
+  a.x = xu.data;
+  a.y = yu.data;
+  a.nd = md.n;
+  a.n = n;
+  for (int m = 0; m < md.n; ++m) {
+    a.ext[m] = md.ext[m];
+    a.ys[m] = md.str[0][m];
+    a.xs[m] = md.str[1][m];
+  }
+  if (md.n == 0) {  // scalar
+    a.nd = 1;
+    a.ext[0] = 1;
+    a.xs[0] = a.ys[0] = 1;
+  }
+  a.sx = sx;
+  a.sy = sy;
+  a.sy_zero = sy_zero;
+  a.sx_one = scalar_is_one(dt, sx);
+  a.tmode = -1;
+  // x's contiguous mode, if it is not y's fastest mode -> tiled transpose
+  int p = -1;
+  for (int m = 0; m < a.nd; ++m)
+    if (a.xs[m] == 1 || a.xs[m] == -1) { p = m; break; }
+  if (p > 0 && (a.xs[0] > 1 || a.xs[0] < -1) && a.ext[0] >= 4 && a.ext[p] >= 4) a.tmode = p;
+  return cuda_err(launch_perm(dt, a, ctx->num_sms, s), "permute kernel");
+}
+
+// ----------------------------------------------------------------------------
+// binary: strided GEMM or index kernel
+// ----------------------------------------------------------------------------
+
+static int reduce_dangling(ome_ctx* ctx, cudaStream_t s, ome_dtype dt, HView& xu, const HView& other,
+                           const HView& yu) {
+  HView r;
+  r.nd = 0;
+  bool any = false;
+  int64_t n = 1;
+  for (int d = 0; d < xu.nd; ++d) {
+    if (find_lab(other, xu.lab[d]) < 0 && find_lab(yu, xu.lab[d]) < 0) {
+      any = true;
+      continue;
+    }
+    r.lab[r.nd] = xu.lab[d];
+    r.ext[r.nd] = xu.ext[d];
+    r.str[r.nd] = n;
+    n *= xu.ext[d];
+    r.nd++;
+  }
+  if (!any) return OME_OK;
+  r.data = static_cast<char*>(ws_alloc(ctx, (size_t)std::max<int64_t>(n, 1) * dtype_size(dt)));
+  if (!r.data)
+    return set_err(OME_OUT_OF_MEMORY, "workspace too small for a dangling-label reduction (%lld elements)",
+                   (long long)n);
+  OME_CK(run_loop(ctx, s, dt, 1, &xu, r, scalar_one(dt), scalar_zero(dt), true));
+  xu = r;
+  return OME_OK;
+}
+
+static int run_binary(ome_ctx* ctx, cudaStream_t s, ome_dtype dt, HView x1, HView x2, const HView& yu,
+                      const Scalar& sx, const Scalar& sy, bool sy_zero, int prec) {
+  OME_CK(reduce_dangling(ctx, s, dt, x1, x2, yu));
+  OME_CK(reduce_dangling(ctx, s, dt, x2, x1, yu));
+  // group tables: M (y, A), N (y, B), K (A, B), L (y, A, B)
+  Modes gm, gn, gk, gl;
+  gm.nt = 2; gn.nt = 2; gk.nt = 2; gl.nt = 3;
+  int64_t st[3];
+  for (int d = 0; d < yu.nd; ++d) {
+    const int32_t l = yu.lab[d];
+    const int k1 = find_lab(x1, l), k2 = find_lab(x2, l);
+    if (k1 >= 0 && k2 >= 0) {
+      st[0] = x1.str[k1]; st[1] = x2.str[k2]; st[2] = yu.str[d];
+      gl.add(yu.ext[d], st);
+    } else if (k2 >= 0) {
+      st[0] = x2.str[k2]; st[1] = yu.str[d];
+      gn.add(yu.ext[d], st);
+    } else {  // in x1 only, or broadcast (stride 0 in A)
+      st[0] = k1 >= 0 ? x1.str[k1] : 0; st[1] = yu.str[d];
+      gm.add(yu.ext[d], st);
+    }
+  }
+  for (int d = 0; d < x1.nd; ++d) {
+    const int32_t l = x1.lab[d];
+    const int k2 = find_lab(x2, l);
+    if (k2 >= 0 && find_lab(yu, l) < 0) {
+      st[0] = x1.str[d]; st[1] = x2.str[k2];
+      gk.add(x1.ext[d], st);
+    }
+  }
+  const int64_t M = gm.total(), N = gn.total(), K = gk.total(), L = gl.total();
+  if (M * N * L == 0) return OME_OK;
+  const bool gemm_shape = M >= 16 && N >= 16 && K >= 8;
+  if (gemm_shape) {
+    gm.normalize(0);
+    gn.normalize(0);
+    // K order: A's contiguous mode first if A is K-contiguous, else B's
+    bool a_kfast = false;
+    for (int i = 0; i < gk.n; ++i)
+      if (gk.str[0][i] == 1) a_kfast = true;
+    gk.normalize(a_kfast ? 0 : 1);
+    gl.normalize(2);
+  }
+  if (gemm_shape && gm.n <= MAXG && gn.n <= MAXG && gk.n <= MAXG && gl.n <= MAXG) {
+    GemmArgs g;
+    memset(&g, 0, sizeof(g));
+    g.A = x1.data;
+    g.B = x2.data;
+    g.C = yu.data;
+    g.M = M; g.N = N; g.K = K; g.L = L;
+    g.nm = gm.n; g.nn = gn.n; g.nk = gk.n; g.nl = gl.n;
+    for (int i = 0; i < gm.n; ++i) { g.m_ext[i] = gm.ext[i]; g.m_sa[i] = gm.str[0][i]; g.m_sc[i] = gm.str[1][i]; }
+    for (int i = 0; i < gn.n; ++i) { g.n_ext[i] = gn.ext[i]; g.n_sb[i] = gn.str[0][i]; g.n_sc[i] = gn.str[1][i]; }
+    for (int i = 0; i < gk.n; ++i) { g.k_ext[i] = gk.ext[i]; g.k_sa[i] = gk.str[0][i]; g.k_sb[i] = gk.str[1][i]; }
+    for (int i = 0; i < gl.n; ++i) {
+      g.l_ext[i] = gl.ext[i]; g.l_sa[i] = gl.str[0][i]; g.l_sb[i] = gl.str[1][i]; g.l_sc[i] = gl.str[2][i];
+    }
+    // empty groups: one unit mode so that offsets evaluate to 0
+    if (g.nm == 0) { g.nm = 1; g.m_ext[0] = 1; }
+    if (g.nn == 0) { g.nn = 1; g.n_ext[0] = 1; }
+    if (g.nk == 0) { g.nk = 1; g.k_ext[0] = 1; }
+    if (g.nl == 0) { g.nl = 1; g.l_ext[0] = 1; }
+    g.a_m_fast = g.m_sa[0] == 1;
+    g.b_n_fast = g.n_sb[0] == 1;
+    g.sx = sx;
+    g.sy = sy;
+    g.sy_zero = sy_zero;
+    g.sx_one = scalar_is_one(dt, sx);
+    if (dt == OME_F32 && prec != OME_PREC_FP32 && gemm_bf16x3_supported(g)) {
+      size_t avail = ctx->ws_bytes > ctx->ws_top ? ctx->ws_bytes - ((ctx->ws_top + 255) & ~(size_t)255) : 0;
+      void* w = avail ? ctx->ws + ((ctx->ws_top + 255) & ~(size_t)255) : nullptr;
+      cudaError_t e = launch_gemm_bf16x3(g, w, avail, ctx->num_sms, s);
+      if (e != cudaErrorNotSupported) return cuda_err(e, "bf16x3 gemm");
+      cudaGetLastError();
+    }
+    return cuda_err(launch_gemm_simt(dt, g, s), "simt gemm");
+  }
+  HView xs[2] = {x1, x2};
+  return run_loop(ctx, s, dt, 2, xs, yu, sx, sy, sy_zero);
+}
+
+// ----------------------------------------------------------------------------
+// einsum on labelled views
+// ----------------------------------------------------------------------------
+
+int einsum_views(ome_ctx* ctx, cudaStream_t s, ome_dtype dt, int nin, const HView* xs, const HView& y,
+                 const Scalar& sx, const Scalar& sy_in, int prec, bool loop_only) {
+  if (nin < 1) return set_err(OME_INVALID_ARGUMENT, "number of input tensors must be greater than 0");
+  if (nin > MAXIN) return set_err(OME_UNSUPPORTED, "at most %d input tensors per contraction", MAXIN);
+  // size dict consistency (get_size_dict!, src/interfaces.jl:75-94)
+  std::vector<std::pair<int32_t, int64_t>> sd;
+  auto check = [&](int32_t l, int64_t e) -> int {
+    for (auto& p : sd)
+      if (p.first == l) {
+        if (p.second != e)
+          return set_err(OME_DIMENSION_MISMATCH, "label %d = %lld or %lld)?", l, (long long)p.second, (long long)e);
+        return OME_OK;
+      }
+    sd.push_back({l, e});
+    return OME_OK;
+  };
+  for (int i = 0; i < nin; ++i)
+    for (int d = 0; d < xs[i].nd; ++d) OME_CK(check(xs[i].lab[d], xs[i].ext[d]));
+  for (int d = 0; d < y.nd; ++d) OME_CK(check(y.lab[d], y.ext[d]));
+
+  HView xu[MAXIN], yu;
+  for (int i = 0; i < nin; ++i) OME_CK(unique_view(xs[i], xu[i]));
+  OME_CK(unique_view(y, yu));
+  if (numel(y) == 0) return OME_OK;
+
+  Scalar sy = sy_in;
+  bool sy_zero = scalar_is_zero(dt, sy);
+  if (scalar_is_zero(dt, sx)) {  // @addmul! iszero(b): y <- sy*y
+    if (!sy_zero && scalar_is_one(dt, sy)) return OME_OK;
+    return cuda_err(launch_scale(dt, y.data, y.nd, y.ext, y.str, sy, sy_zero, ctx->num_sms, s), "scale");
+  }
+  if (yu.nd < y.nd) {
+    // repeated output labels: off-diagonal entries <- sy*y (or zero); the
+    // diagonal view then accumulates onto the scaled values.
+    if (!(!sy_zero && scalar_is_one(dt, sy)))
+      OME_CK(cuda_err(launch_scale(dt, y.data, y.nd, y.ext, y.str, sy, sy_zero, ctx->num_sms, s), "scale"));
+    sy = scalar_one(dt);
+  }
+  if (loop_only || nin >= 3) return run_loop(ctx, s, dt, nin, xu, yu, sx, sy, sy_zero);
+  if (nin == 1) return run_unary(ctx, s, dt, xu[0], yu, sx, sy, sy_zero);
+  return run_binary(ctx, s, dt, xu[0], xu[1], yu, sx, sy, sy_zero, prec);
+}
+
+}  // namespace ome
+
+using namespace ome;
+
+// ============================================================================
+// C ABI
+// ============================================================================
+
+extern "C" {
+
+int ome_version(void) { return 1; }
+
+unsigned long long ome_launch_count(void) { return ome::launch_counter(); }
+
+const char* ome_last_error(void) { return g_err.c_str(); }
+
+int ome_ctx_create(int device, size_t workspace_bytes, ome_ctx** out) {
+  if (!out) return set_err(OME_INVALID_ARGUMENT, "out is NULL");
+  *out = nullptr;
+  int ndev = 0;
+  OME_CUDA(cudaGetDeviceCount(&ndev), "cudaGetDeviceCount");
+  if (device < 0 || device >= ndev) return set_err(OME_INVALID_ARGUMENT, "device %d of %d", device, ndev);
+  OME_CUDA(cudaSetDevice(device), "cudaSetDevice");
+  ome_ctx* c = new ome_ctx();
+  c->device = device;
+  cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, device);
+  c->ws = nullptr;
+  c->ws_bytes = workspace_bytes;
+  c->ws_top = 0;
+  if (workspace_bytes) {
+    cudaError_t e = cudaMalloc(&c->ws, workspace_bytes);
+    if (e != cudaSuccess) {
+      delete c;
+      return cuda_err(e, "workspace cudaMalloc");
+    }
+  }
+  *out = c;
+  return OME_OK;
+}
+
+int ome_ctx_destroy(ome_ctx* ctx) {
+  if (!ctx) return OME_OK;
+  if (ctx->ws) cudaFree(ctx->ws);
+  delete ctx;
+  return OME_OK;
+}
+
+int ome_ctx_workspace_bytes(const ome_ctx* ctx, size_t* out) {
+  if (!ctx || !out) return set_err(OME_INVALID_ARGUMENT, "NULL argument");
+  *out = ctx->ws_bytes;
+  return OME_OK;
+}
+
+static int einsum_entry(ome_ctx* ctx, void* stream, ome_dtype dtype, int32_t ninputs, const ome_tensor* xs,
+                        const ome_tensor* y, const void* sx, const void* sy, int32_t prec, bool loop_only) {
+  if (!ctx || !y || !sx || !sy || (ninputs > 0 && !xs)) return set_err(OME_INVALID_ARGUMENT, "NULL argument");
+  if ((int)dtype < 0 || (int)dtype > OME_TROP_F64) return set_err(OME_INVALID_ARGUMENT, "unknown dtype %d", (int)dtype);
+  if (ninputs < 1) return set_err(OME_INVALID_ARGUMENT, "number of input tensors must be greater than 0");
+  if (ninputs > MAXIN) return set_err(OME_UNSUPPORTED, "at most %d input tensors per contraction", MAXIN);
+  HView xv[MAXIN], yv;
+  for (int i = 0; i < ninputs; ++i) OME_CK(view_from_tensor(xs[i], xv[i], "input"));
+  OME_CK(view_from_tensor(*y, yv, "output"));
+  ctx->ws_top = 0;
+  return einsum_views(ctx, static_cast<cudaStream_t>(stream), dtype, ninputs, xv, yv, scalar_from(dtype, sx),
+                      scalar_from(dtype, sy), prec, loop_only);
+}
+
+int ome_einsum(ome_ctx* ctx, void* stream, ome_dtype dtype, int32_t ninputs, const ome_tensor* xs,
+               const ome_tensor* y, const void* sx, const void* sy, int32_t prec) {
+  return einsum_entry(ctx, stream, dtype, ninputs, xs, y, sx, sy, prec, false);
+}
+
+int ome_loop_einsum(ome_ctx* ctx, void* stream, ome_dtype dtype, int32_t ninputs, const ome_tensor* xs,
+                    const ome_tensor* y, const void* sx, const void* sy) {
+  return einsum_entry(ctx, stream, dtype, ninputs, xs, y, sx, sy, OME_PREC_FP32, true);
+}
+
+}  // extern "C"

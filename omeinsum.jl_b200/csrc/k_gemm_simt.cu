@@ -1,0 +1,165 @@
+// CUDA-core strided batched GEMM over any algebra.
+//
+// Replaces analyze_binary's permute -> reshape -> (batched) GEMM chain
+// (src/einsum.jl:104-124, src/binaryrules.jl:46-61,94-141, src/utils.jl:162-177,
+// ext/CUDAExt.jl:115-117,156-178) for the element types that have no
+// tensor-core path (Int64, Bool, tropical, FP64, complex) and for the plain
+// FP32 comparison path.  Operands are read in place through per-group mode
+// strides, so no permuted copy is ever materialised; the output permutation
+// is absorbed in the epilogue's strides.
+#include <string.h>
+#include "kernels.h"
+
+namespace ome {
+
+template <int ES> struct SimtCfg;                 // by element size
+template <> struct SimtCfg<1> { static constexpr int BM = 128, BN = 128, BK = 8, TM = 8, TN = 8; };
+template <> struct SimtCfg<4> { static constexpr int BM = 128, BN = 128, BK = 8, TM = 8, TN = 8; };
+template <> struct SimtCfg<8> { static constexpr int BM = 64, BN = 64, BK = 8, TM = 4, TN = 4; };
+template <> struct SimtCfg<16> { static constexpr int BM = 64, BN = 64, BK = 8, TM = 4, TN = 4; };
+
+__device__ __forceinline__ int64_t group_off(int64_t i, int n, const int64_t* ext, const int64_t* str) {
+  if (n == 1) return i * str[0];
+  return mode_offset(i, n, ext, str);
+}
+
+template <class A>
+__global__ void __launch_bounds__(256) k_gemm_simt(const __grid_constant__ GemmArgs g) {
+  using T = typename A::T;
+  using C = SimtCfg<sizeof(T)>;
+  constexpr int BM = C::BM, BN = C::BN, BK = C::BK, TM = C::TM, TN = C::TN;
+  constexpr int NT = 256;
+  constexpr int RA = BM * BK / NT, RB = BN * BK / NT;
+  static_assert((BM / TM) * (BN / TN) == NT, "thread tile");
+  __shared__ T As[2][BK][BM];
+  __shared__ T Bs[2][BK][BN];
+  __shared__ int64_t am[BM], bn[BN];
+
+  const T* Ap = static_cast<const T*>(g.A);
+  const T* Bp = static_cast<const T*>(g.B);
+  T* Cp = static_cast<T*>(g.C);
+  const T sx = scalar_as<T>(g.sx), sy = scalar_as<T>(g.sy);
+  const int tid = threadIdx.x;
+  const int tx = tid % (BN / TN), ty = tid / (BN / TN);
+  const int64_t m0 = (int64_t)blockIdx.x * BM, n0 = (int64_t)blockIdx.y * BN;
+
+  for (int64_t l = blockIdx.z; l < g.L; l += gridDim.z) {
+    const int64_t la = mode_offset(l, g.nl, g.l_ext, g.l_sa);
+    const int64_t lb = mode_offset(l, g.nl, g.l_ext, g.l_sb);
+    const int64_t lc = mode_offset(l, g.nl, g.l_ext, g.l_sc);
+    for (int i = tid; i < BM; i += NT)
+      am[i] = (m0 + i < g.M) ? la + group_off(m0 + i, g.nm, g.m_ext, g.m_sa) : -1;
+    for (int i = tid; i < BN; i += NT)
+      bn[i] = (n0 + i < g.N) ? lb + group_off(n0 + i, g.nn, g.n_ext, g.n_sb) : -1;
+    __syncthreads();
+
+    T acc[TM][TN];
+#pragma unroll
+    for (int i = 0; i < TM; ++i)
+#pragma unroll
+      for (int j = 0; j < TN; ++j) acc[i][j] = A::zero();
+
+    T ra[RA], rb[RB];
+    auto load = [&](int64_t k0) {
+#pragma unroll
+      for (int r = 0; r < RA; ++r) {
+        const int e = tid + NT * r;
+        const int mm = g.a_m_fast ? e % BM : e / BK;
+        const int kk = g.a_m_fast ? e / BM : e % BK;
+        const int64_t k = k0 + kk;
+        const int64_t base = am[mm];
+        ra[r] = (base >= 0 && k < g.K) ? Ap[base + group_off(k, g.nk, g.k_ext, g.k_sa)] : A::zero();
+      }
+#pragma unroll
+      for (int r = 0; r < RB; ++r) {
+        const int e = tid + NT * r;
+        const int nn = g.b_n_fast ? e % BN : e / BK;
+        const int kk = g.b_n_fast ? e / BN : e % BK;
+        const int64_t k = k0 + kk;
+        const int64_t base = bn[nn];
+        rb[r] = (base >= 0 && k < g.K) ? Bp[base + group_off(k, g.nk, g.k_ext, g.k_sb)] : A::zero();
+      }
+    };
+    auto store = [&](int buf) {
+#pragma unroll
+      for (int r = 0; r < RA; ++r) {
+        const int e = tid + NT * r;
+        const int mm = g.a_m_fast ? e % BM : e / BK;
+        const int kk = g.a_m_fast ? e / BM : e % BK;
+        As[buf][kk][mm] = ra[r];
+      }
+#pragma unroll
+      for (int r = 0; r < RB; ++r) {
+        const int e = tid + NT * r;
+        const int nn = g.b_n_fast ? e % BN : e / BK;
+        const int kk = g.b_n_fast ? e / BN : e % BK;
+        Bs[buf][kk][nn] = rb[r];
+      }
+    };
+
+    load(0);
+    store(0);
+    __syncthreads();
+    int buf = 0;
+    for (int64_t k0 = 0; k0 < g.K; k0 += BK) {
+      const bool more = k0 + BK < g.K;
+      if (more) load(k0 + BK);
+#pragma unroll
+      for (int kk = 0; kk < BK; ++kk) {
+        T a[TM], b[TN];
+#pragma unroll
+        for (int i = 0; i < TM; ++i) a[i] = As[buf][kk][ty * TM + i];
+#pragma unroll
+        for (int j = 0; j < TN; ++j) b[j] = Bs[buf][kk][tx * TN + j];
+#pragma unroll
+        for (int i = 0; i < TM; ++i)
+#pragma unroll
+          for (int j = 0; j < TN; ++j) acc[i][j] = A::fma(a[i], b[j], acc[i][j]);
+      }
+      if (more) store(buf ^ 1);
+      __syncthreads();
+      buf ^= 1;
+    }
+
+    int64_t cm[TM], cn[TN];
+#pragma unroll
+    for (int i = 0; i < TM; ++i) {
+      const int64_t m = m0 + ty * TM + i;
+      cm[i] = m < g.M ? group_off(m, g.nm, g.m_ext, g.m_sc) : -1;
+    }
+#pragma unroll
+    for (int j = 0; j < TN; ++j) {
+      const int64_t n = n0 + tx * TN + j;
+      cn[j] = n < g.N ? group_off(n, g.nn, g.n_ext, g.n_sc) : -1;
+    }
+#pragma unroll
+    for (int i = 0; i < TM; ++i)
+#pragma unroll
+      for (int j = 0; j < TN; ++j)
+        if (cm[i] >= 0 && cn[j] >= 0) {
+          T* cp = Cp + lc + cm[i] + cn[j];
+          *cp = epilogue<A>(acc[i][j], cp, sx, sy, g.sy_zero, g.sx_one);
+        }
+    __syncthreads();
+  }
+}
+
+template <class A>
+static cudaError_t launch_gemm_simt_t(const GemmArgs& g, cudaStream_t s) {
+  using C = SimtCfg<sizeof(typename A::T)>;
+  const int64_t gm = (g.M + C::BM - 1) / C::BM, gn = (g.N + C::BN - 1) / C::BN;
+  if (gm > 0x7fffffff || gn > 65535) return cudaErrorNotSupported;
+  const int64_t gl = g.L < 65535 ? g.L : 65535;
+  dim3 grid((unsigned)gm, (unsigned)gn, (unsigned)gl);
+  k_gemm_simt<A><<<grid, 256, 0, s>>>(g); count_launch();
+  return cudaGetLastError();
+}
+
+cudaError_t launch_gemm_simt(ome_dtype dt, const GemmArgs& g, cudaStream_t s) {
+  if (g.M == 0 || g.N == 0 || g.L == 0) return cudaSuccess;
+  cudaError_t e = cudaErrorInvalidValue;
+  OME_DISPATCH(dt, ALG, e = launch_gemm_simt_t<ALG>(g, s));
+  return e;
+}
+
+}  // namespace ome

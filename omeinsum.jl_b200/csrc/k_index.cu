@@ -1,0 +1,583 @@
+// Index-iterating kernels of libomeb200:
+//  * k_loop_thread / k_loop_block / k_loop_finish: the generic sum-product
+//    over labelled strided inputs (loop_einsum!, src/loop_einsum.jl:21-45;
+//    GPU form ext/CUDAExt.jl:60-113).  Also serves Sum (src/unaryrules.jl:30-40),
+//    Tr (:22-26) on a diagonal view, GEMV/dot/outer/Hadamard-shaped binary
+//    rules and the n-ary fallback.
+//  * k_transpose / k_copy: Permutedims via tensorpermute! (src/utils.jl:122-156),
+//    Repeat (src/unaryrules.jl:44-58, stride-0 input modes) and Identity.
+//  * k_scale, k_acc64*: αβ pre-pass and FP64 cross-slice accumulation.
+#include <string.h>
+#include "kernels.h"
+
+namespace ome {
+
+static unsigned long long g_launches = 0;
+unsigned long long launch_counter() { return __atomic_load_n(&g_launches, __ATOMIC_RELAXED); }
+void count_launch(int n) { __atomic_fetch_add(&g_launches, (unsigned long long)n, __ATOMIC_RELAXED); }
+
+// ---------------------------------------------------------------------------
+// generic loop kernel
+// ---------------------------------------------------------------------------
+
+template <class A, int NIN>
+__device__ __forceinline__ typename A::T loop_prod(const LoopArgs& a, const int64_t* off) {
+  using T = typename A::T;
+  const int nin = NIN > 0 ? NIN : a.nin;
+  T p = static_cast<const T*>(a.x[0])[off[0]];
+#pragma unroll
+  for (int i = 1; i < (NIN > 0 ? NIN : MAXIN); ++i) {
+    if (i < nin) p = A::mul(p, static_cast<const T*>(a.x[i])[off[i]]);
+  }
+  return p;
+}
+
+// Decompose output index o over the output modes; fills input offsets.
+template <int NIN>
+__device__ __forceinline__ int64_t loop_outer_offsets(const LoopArgs& a, int64_t o, int64_t* off) {
+  const int nin = NIN > 0 ? NIN : a.nin;
+  int64_t yoff = 0;
+#pragma unroll
+  for (int i = 0; i < (NIN > 0 ? NIN : MAXIN); ++i) off[i] = 0;
+  for (int m = 0; m < a.nout; ++m) {
+    const int64_t e = a.ext[m];
+    const int64_t q = o / e;
+    const int64_t d = o - q * e;
+    o = q;
+    yoff += d * a.str[0][m];
+#pragma unroll
+    for (int i = 0; i < (NIN > 0 ? NIN : MAXIN); ++i)
+      if (i < nin) off[i] += d * a.str[1 + i][m];
+  }
+  return yoff;
+}
+
+// One thread per output element; the first inner mode is a plain loop, the
+// remaining inner modes an odometer (no divisions in the inner loop).
+template <class A, int NIN>
+__global__ void __launch_bounds__(256) k_loop_thread(const __grid_constant__ LoopArgs a) {
+  using T = typename A::T;
+  constexpr int NI = NIN > 0 ? NIN : MAXIN;
+  const int nin = NIN > 0 ? NIN : a.nin;
+  const T sx = scalar_as<T>(a.sx), sy = scalar_as<T>(a.sy);
+  const int m0 = a.nout;
+  const int64_t e0 = a.ninner > 0 ? a.ext[m0] : 1;
+  for (int64_t o = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; o < a.n_out;
+       o += (int64_t)gridDim.x * blockDim.x) {
+    int64_t off[NI];
+    const int64_t yoff = loop_outer_offsets<NIN>(a, o, off);
+    T acc = A::zero();
+    if (a.n_in > 0) {
+      int64_t s0[NI];
+#pragma unroll
+      for (int i = 0; i < NI; ++i) s0[i] = (i < nin && a.ninner > 0) ? a.str[1 + i][m0] : 0;
+      int dig[MAXM];
+      for (int m = 0; m < a.ninner; ++m) dig[m] = 0;
+      while (true) {
+        int64_t o2[NI];
+#pragma unroll
+        for (int i = 0; i < NI; ++i) o2[i] = off[i];
+        for (int64_t j = 0; j < e0; ++j) {
+          acc = A::add(acc, loop_prod<A, NIN>(a, o2));
+#pragma unroll
+          for (int i = 0; i < NI; ++i) o2[i] += s0[i];
+        }
+        int m = 1;
+        for (; m < a.ninner; ++m) {
+          const int mm = m0 + m;
+          dig[m]++;
+#pragma unroll
+          for (int i = 0; i < NI; ++i)
+            if (i < nin) off[i] += a.str[1 + i][mm];
+          if (dig[m] < a.ext[mm]) break;
+#pragma unroll
+          for (int i = 0; i < NI; ++i)
+            if (i < nin) off[i] -= a.ext[mm] * a.str[1 + i][mm];
+          dig[m] = 0;
+        }
+        if (m >= a.ninner) break;
+      }
+    }
+    T* yp = static_cast<T*>(a.y) + yoff;
+    *yp = epilogue<A>(acc, yp, sx, sy, a.sy_zero, a.sx_one);
+  }
+}
+
+// Inner counter advanced by a fixed step given as mixed-radix digits.
+template <int NIN>
+struct InnerCursor {
+  int64_t dig[MAXM];
+  __device__ __forceinline__ void init(const LoopArgs& a, int64_t j, int64_t* off) {
+    const int nin = NIN > 0 ? NIN : a.nin;
+    for (int m = 0; m < a.ninner; ++m) {
+      const int mm = a.nout + m;
+      const int64_t e = a.ext[mm];
+      const int64_t q = j / e;
+      const int64_t d = j - q * e;
+      j = q;
+      dig[m] = d;
+#pragma unroll
+      for (int i = 0; i < (NIN > 0 ? NIN : MAXIN); ++i)
+        if (i < nin) off[i] += d * a.str[1 + i][mm];
+    }
+  }
+  __device__ __forceinline__ void advance(const LoopArgs& a, int64_t* off) {
+    const int nin = NIN > 0 ? NIN : a.nin;
+    int carry = 0;
+    for (int m = 0; m < a.ninner; ++m) {
+      const int mm = a.nout + m;
+      int64_t nd = dig[m] + a.stepdig[m] + carry;
+      const int64_t e = a.ext[mm];
+      carry = nd >= e;
+      if (carry) nd -= e;
+      const int64_t delta = nd - dig[m];
+      dig[m] = nd;
+#pragma unroll
+      for (int i = 0; i < (NIN > 0 ? NIN : MAXIN); ++i)
+        if (i < nin) off[i] += delta * a.str[1 + i][mm];
+    }
+  }
+};
+
+// One block per output element (nsplit == 1), or nsplit blocks per output
+// each summing a strided share of the inner space into a.partial.
+template <class A, int NIN>
+__global__ void __launch_bounds__(256) k_loop_block(const __grid_constant__ LoopArgs a) {
+  using T = typename A::T;
+  constexpr int NI = NIN > 0 ? NIN : MAXIN;
+  constexpr int U = 4;
+  __shared__ T sh[32];
+  const T sx = scalar_as<T>(a.sx), sy = scalar_as<T>(a.sy);
+  const int64_t step = (int64_t)blockDim.x * a.nsplit;
+  const int64_t nblocks = a.n_out * a.nsplit;
+  for (int64_t b = blockIdx.x; b < nblocks; b += gridDim.x) {
+    const int64_t o = b / a.nsplit;
+    const int64_t split = b - o * a.nsplit;
+    int64_t off[NI];
+    const int64_t yoff = loop_outer_offsets<NIN>(a, o, off);
+    T acc = A::zero();
+    int64_t j = split * blockDim.x + threadIdx.x;
+    if (j < a.n_in) {
+      InnerCursor<NIN> cur;
+      cur.init(a, j, off);
+      while (j < a.n_in) {
+        T v[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+          if (j < a.n_in) {
+            v[u] = loop_prod<A, NIN>(a, off);
+            j += step;
+            if (j < a.n_in) cur.advance(a, off);
+          } else {
+            v[u] = A::zero();
+          }
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u) acc = A::add(acc, v[u]);
+      }
+    }
+    acc = block_reduce<A>(acc, sh);
+    if (threadIdx.x == 0) {
+      if (a.nsplit == 1) {
+        T* yp = static_cast<T*>(a.y) + yoff;
+        *yp = epilogue<A>(acc, yp, sx, sy, a.sy_zero, a.sx_one);
+      } else {
+        static_cast<T*>(a.partial)[b] = acc;
+      }
+    }
+  }
+}
+
+// Sum the nsplit partials of each output in a fixed order and apply the αβ
+// epilogue (deterministic two-pass reduction).
+template <class A>
+__global__ void __launch_bounds__(256) k_loop_finish(const __grid_constant__ LoopArgs a) {
+  using T = typename A::T;
+  const T sx = scalar_as<T>(a.sx), sy = scalar_as<T>(a.sy);
+  for (int64_t o = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; o < a.n_out;
+       o += (int64_t)gridDim.x * blockDim.x) {
+    int64_t yoff = 0, r = o;
+    for (int m = 0; m < a.nout; ++m) {
+      const int64_t e = a.ext[m];
+      const int64_t q = r / e;
+      yoff += (r - q * e) * a.str[0][m];
+      r = q;
+    }
+    const T* p = static_cast<const T*>(a.partial) + o * a.nsplit;
+    T acc = A::zero();
+    for (int s = 0; s < a.nsplit; ++s) acc = A::add(acc, p[s]);
+    T* yp = static_cast<T*>(a.y) + yoff;
+    *yp = epilogue<A>(acc, yp, sx, sy, a.sy_zero, a.sx_one);
+  }
+}
+
+template <class A>
+static cudaError_t launch_loop_t(const LoopArgs& a, LoopMode mode, int grid, int block,
+                                 cudaStream_t s) {
+  if (mode == LOOP_THREAD) {
+    switch (a.nin) {
+      case 1: k_loop_thread<A, 1><<<grid, block, 0, s>>>(a); count_launch(); break;
+      case 2: k_loop_thread<A, 2><<<grid, block, 0, s>>>(a); count_launch(); break;
+      case 3: k_loop_thread<A, 3><<<grid, block, 0, s>>>(a); count_launch(); break;
+      default: k_loop_thread<A, 0><<<grid, block, 0, s>>>(a); count_launch(); break;
+    }
+  } else {
+    switch (a.nin) {
+      case 1: k_loop_block<A, 1><<<grid, block, 0, s>>>(a); count_launch(); break;
+      case 2: k_loop_block<A, 2><<<grid, block, 0, s>>>(a); count_launch(); break;
+      case 3: k_loop_block<A, 3><<<grid, block, 0, s>>>(a); count_launch(); break;
+      default: k_loop_block<A, 0><<<grid, block, 0, s>>>(a); count_launch(); break;
+    }
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t launch_loop(ome_dtype dt, const LoopArgs& a, LoopMode mode, int grid, int block,
+                        cudaStream_t s) {
+  cudaError_t e = cudaErrorInvalidValue;
+  OME_DISPATCH(dt, ALG, e = launch_loop_t<ALG>(a, mode, grid, block, s));
+  return e;
+}
+
+cudaError_t launch_loop_finish(ome_dtype dt, const LoopArgs& a, cudaStream_t s) {
+  const int64_t nb = (a.n_out + 255) / 256;
+  const int grid = (int)(nb < 4096 ? nb : 4096);
+  cudaError_t e = cudaErrorInvalidValue;
+  OME_DISPATCH(dt, ALG, k_loop_finish<ALG><<<grid, 256, 0, s>>>(a); count_launch(); e = cudaGetLastError());
+  return e;
+}
+
+// ---------------------------------------------------------------------------
+// permute / broadcast copy
+// ---------------------------------------------------------------------------
+
+// 32x32 tile transpose between y's fastest mode (mode 0) and x's fastest
+// mode (tmode); every other mode is a batch index.  Reads are coalesced
+// along x's contiguous mode, writes along y's.  256 threads = 32 x 8.
+template <class A>
+__global__ void __launch_bounds__(256) k_transpose(const __grid_constant__ PermArgs a) {
+  using T = typename A::T;
+  __shared__ T tile[32][33];
+  const T sx = scalar_as<T>(a.sx), sy = scalar_as<T>(a.sy);
+  const int tmode = a.tmode;
+  const int64_t e0 = a.ext[0], et = a.ext[tmode];
+  const int64_t t0 = (e0 + 31) >> 5, tt = (et + 31) >> 5;
+  const int64_t nbatch = a.n / (e0 * et);
+  const int64_t ntiles = t0 * tt * nbatch;
+  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+  const T* x = static_cast<const T*>(a.x);
+  T* y = static_cast<T*>(a.y);
+  for (int64_t tid = blockIdx.x; tid < ntiles; tid += gridDim.x) {
+    int64_t r = tid;
+    const int64_t i0 = r % t0;
+    r /= t0;
+    const int64_t it = r % tt;
+    r /= tt;
+    int64_t xb = 0, yb = 0;
+    for (int m = 1; m < a.nd; ++m) {
+      if (m == tmode) continue;
+      const int64_t e = a.ext[m];
+      const int64_t q = r / e;
+      const int64_t d = r - q * e;
+      r = q;
+      xb += d * a.xs[m];
+      yb += d * a.ys[m];
+    }
+    const int64_t p = it * 32 + tx;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const int64_t q = i0 * 32 + ty + 8 * k;
+      if (p < et && q < e0) tile[ty + 8 * k][tx] = x[xb + p * a.xs[tmode] + q * a.xs[0]];
+    }
+    __syncthreads();
+    const int64_t q = i0 * 32 + tx;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const int64_t pp = it * 32 + ty + 8 * k;
+      if (pp < et && q < e0) {
+        T* yp = y + yb + q * a.ys[0] + pp * a.ys[tmode];
+        *yp = epilogue<A>(tile[tx][ty + 8 * k], yp, sx, sy, a.sy_zero, a.sx_one);
+      }
+    }
+    __syncthreads();
+  }
+}
+
+// Elementwise copy in y order (x's fastest mode is y's, or x is broadcast).
+template <class A>
+__global__ void __launch_bounds__(256) k_copy(const __grid_constant__ PermArgs a) {
+  using T = typename A::T;
+  const T sx = scalar_as<T>(a.sx), sy = scalar_as<T>(a.sy);
+  const T* x = static_cast<const T*>(a.x);
+  T* y = static_cast<T*>(a.y);
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < a.n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    int64_t r = i, xo = 0, yo = 0;
+    for (int m = 0; m < a.nd; ++m) {
+      const int64_t e = a.ext[m];
+      const int64_t q = r / e;
+      const int64_t d = r - q * e;
+      r = q;
+      xo += d * a.xs[m];
+      yo += d * a.ys[m];
+    }
+    T* yp = y + yo;
+    *yp = epilogue<A>(x[xo], yp, sx, sy, a.sy_zero, a.sx_one);
+  }
+}
+
+// Contiguous 1-mode copy with 16-byte vectors (both unit stride, aligned).
+template <class A>
+__global__ void __launch_bounds__(256) k_copy_vec(const __grid_constant__ PermArgs a) {
+  using T = typename A::T;
+  constexpr int V = 16 / sizeof(T);
+  const T sx = scalar_as<T>(a.sx), sy = scalar_as<T>(a.sy);
+  const int64_t nv = a.n / V;
+  const uint4* x = static_cast<const uint4*>(a.x);
+  uint4* y = static_cast<uint4*>(a.y);
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < nv;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    uint4 xv = x[i];
+    if (!(a.sx_one && a.sy_zero)) {
+      uint4 yv;
+      if (!a.sy_zero) yv = y[i];
+      T* xe = reinterpret_cast<T*>(&xv);
+      T* ye = reinterpret_cast<T*>(&yv);
+#pragma unroll
+      for (int v = 0; v < V; ++v) xe[v] = epilogue<A>(xe[v], ye + v, sx, sy, a.sy_zero, a.sx_one);
+    }
+    y[i] = xv;
+  }
+  // tail
+  const T* xs = static_cast<const T*>(a.x);
+  T* ys = static_cast<T*>(a.y);
+  for (int64_t i = nv * V + blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < a.n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    ys[i] = epilogue<A>(xs[i], ys + i, sx, sy, a.sy_zero, a.sx_one);
+  }
+}
+
+template <class A>
+static cudaError_t launch_perm_t(const PermArgs& a, int num_sms, cudaStream_t s) {
+  using T = typename A::T;
+  if (a.n == 0) return cudaSuccess;
+  const int maxgrid = num_sms * 16;
+  if (a.tmode > 0) {
+    const int64_t tiles = ((a.ext[0] + 31) / 32) * ((a.ext[a.tmode] + 31) / 32) *
+                          (a.n / (a.ext[0] * a.ext[a.tmode]));
+    const int grid = (int)(tiles < maxgrid ? tiles : maxgrid);
+    k_transpose<A><<<grid, 256, 0, s>>>(a); count_launch();
+  } else if (a.nd == 1 && a.xs[0] == 1 && a.ys[0] == 1 && sizeof(T) <= 16 && 16 % sizeof(T) == 0 &&
+             ((uintptr_t)a.x % 16) == 0 && ((uintptr_t)a.y % 16) == 0) {
+    const int64_t nb = (a.n / (16 / sizeof(T)) + 255) / 256;
+    const int grid = (int)(nb < 1 ? 1 : (nb < maxgrid ? nb : maxgrid));
+    k_copy_vec<A><<<grid, 256, 0, s>>>(a); count_launch();
+  } else {
+    const int64_t nb = (a.n + 255) / 256;
+    const int grid = (int)(nb < maxgrid ? nb : maxgrid);
+    k_copy<A><<<grid, 256, 0, s>>>(a); count_launch();
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t launch_perm(ome_dtype dt, const PermArgs& a, int num_sms, cudaStream_t s) {
+  cudaError_t e = cudaErrorInvalidValue;
+  OME_DISPATCH(dt, ALG, e = launch_perm_t<ALG>(a, num_sms, s));
+  return e;
+}
+
+// ---------------------------------------------------------------------------
+// scale pre-pass (outputs with repeated labels)
+// ---------------------------------------------------------------------------
+
+template <class A>
+__global__ void __launch_bounds__(256) k_scale(const __grid_constant__ PermArgs a) {
+  using T = typename A::T;
+  const T sy = scalar_as<T>(a.sy);
+  T* y = static_cast<T*>(a.y);
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < a.n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    int64_t r = i, yo = 0;
+    for (int m = 0; m < a.nd; ++m) {
+      const int64_t e = a.ext[m];
+      const int64_t q = r / e;
+      yo += (r - q * e) * a.ys[m];
+      r = q;
+    }
+    y[yo] = a.sy_zero ? A::zero() : A::mul(sy, y[yo]);
+  }
+}
+
+cudaError_t launch_scale(ome_dtype dt, void* y, int nd, const int64_t* ext, const int64_t* str,
+                         const Scalar& sy, int sy_zero, int num_sms, cudaStream_t s) {
+  PermArgs a;
+  memset(&a, 0, sizeof(a));
+  a.y = y;
+  a.nd = nd;
+  a.n = 1;
+  for (int m = 0; m < nd; ++m) {
+    a.ext[m] = ext[m];
+    a.ys[m] = str[m];
+    a.n *= ext[m];
+  }
+  a.sy = sy;
+  a.sy_zero = sy_zero;
+  if (a.n == 0) return cudaSuccess;
+  const int64_t nb = (a.n + 255) / 256;
+  const int maxgrid = num_sms * 16;
+  const int grid = (int)(nb < maxgrid ? nb : maxgrid);
+  cudaError_t e = cudaErrorInvalidValue;
+  OME_DISPATCH(dt, ALG, k_scale<ALG><<<grid, 256, 0, s>>>(a); count_launch(); e = cudaGetLastError());
+  return e;
+}
+
+// ---------------------------------------------------------------------------
+// FP64 cross-slice accumulation
+// ---------------------------------------------------------------------------
+
+template <class T, class W>
+__global__ void __launch_bounds__(256) k_acc64(W* acc, const T* src, int64_t n) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    acc[i] += (W)src[i];
+}
+__global__ void __launch_bounds__(256) k_acc64_c(double2* acc, const cf32* src, int64_t n) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    acc[i].x += (double)src[i].re;
+    acc[i].y += (double)src[i].im;
+  }
+}
+
+cudaError_t launch_acc64(ome_dtype dt, void* acc, const void* src, int64_t n, cudaStream_t s) {
+  const int64_t nb = (n + 255) / 256;
+  const int grid = (int)(nb < 2048 ? (nb < 1 ? 1 : nb) : 2048);
+  switch (dt) {
+    case OME_F32: k_acc64<float, double><<<grid, 256, 0, s>>>((double*)acc, (const float*)src, n); count_launch(); break;
+    case OME_F64: k_acc64<double, double><<<grid, 256, 0, s>>>((double*)acc, (const double*)src, n); count_launch(); break;
+    case OME_C32: k_acc64_c<<<grid, 256, 0, s>>>((double2*)acc, (const cf32*)src, n); count_launch(); break;
+    default: return cudaErrorInvalidValue;
+  }
+  return cudaGetLastError();
+}
+
+template <class A, class W>
+__global__ void __launch_bounds__(256) k_acc64_store(typename A::T* y, const W* acc, int64_t n,
+                                                     Scalar sxs, Scalar sys, int sy_zero) {
+  using T = typename A::T;
+  const T sx = scalar_as<T>(sxs), sy = scalar_as<T>(sys);
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    T f;
+    if constexpr (sizeof(W) == 16) {
+      f.re = (decltype(f.re))acc[i].x;
+      f.im = (decltype(f.im))acc[i].y;
+    } else {
+      f = (T)acc[i];
+    }
+    y[i] = epilogue<A>(f, y + i, sx, sy, sy_zero, false);
+  }
+}
+
+cudaError_t launch_acc64_store(ome_dtype dt, void* y, const void* acc, int64_t n, const Scalar& sx,
+                               const Scalar& sy, int sy_zero, cudaStream_t s) {
+  const int64_t nb = (n + 255) / 256;
+  const int grid = (int)(nb < 2048 ? (nb < 1 ? 1 : nb) : 2048);
+  switch (dt) {
+    case OME_F32:
+      k_acc64_store<AlgF32, double><<<grid, 256, 0, s>>>((float*)y, (const double*)acc, n, sx, sy, sy_zero); count_launch();
+      break;
+    case OME_F64:
+      k_acc64_store<AlgF64, double><<<grid, 256, 0, s>>>((double*)y, (const double*)acc, n, sx, sy, sy_zero); count_launch();
+      break;
+    case OME_C32:
+      k_acc64_store<AlgC32, double2><<<grid, 256, 0, s>>>((cf32*)y, (const double2*)acc, n, sx, sy, sy_zero); count_launch();
+      break;
+    default: return cudaErrorInvalidValue;
+  }
+  return cudaGetLastError();
+}
+
+template <class W, class T>
+__global__ void __launch_bounds__(256) k_acc64_strided(char* acc, const T* src, PermArgs a) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < a.n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    int64_t r = i, yo = 0;
+    for (int m = 0; m < a.nd; ++m) {
+      const int64_t e = a.ext[m];
+      const int64_t q = r / e;
+      yo += (r - q * e) * a.ys[m];
+      r = q;
+    }
+    W* w = reinterpret_cast<W*>(acc) + yo;
+    if constexpr (sizeof(W) == 16) {
+      w->x += (double)src[i].re;
+      w->y += (double)src[i].im;
+    } else {
+      *w += (double)src[i];
+    }
+  }
+}
+
+cudaError_t launch_acc64_strided(ome_dtype dt, void* acc, const void* src, int nd, const int64_t* ext,
+                                 const int64_t* acc_str, cudaStream_t s) {
+  PermArgs a;
+  memset(&a, 0, sizeof(a));
+  a.nd = nd;
+  a.n = 1;
+  for (int m = 0; m < nd; ++m) {
+    a.ext[m] = ext[m];
+    a.ys[m] = acc_str[m];
+    a.n *= ext[m];
+  }
+  if (a.n == 0) return cudaSuccess;
+  const int64_t nb = (a.n + 255) / 256;
+  const int grid = (int)(nb < 2048 ? nb : 2048);
+  switch (dt) {
+    case OME_F32: k_acc64_strided<double, float><<<grid, 256, 0, s>>>((char*)acc, (const float*)src, a); count_launch(); break;
+    case OME_F64: k_acc64_strided<double, double><<<grid, 256, 0, s>>>((char*)acc, (const double*)src, a); count_launch(); break;
+    case OME_C32: k_acc64_strided<double2, cf32><<<grid, 256, 0, s>>>((char*)acc, (const cf32*)src, a); count_launch(); break;
+    default: return cudaErrorInvalidValue;
+  }
+  return cudaGetLastError();
+}
+
+template <class T>
+__global__ void __launch_bounds__(256) k_conj(T* x, int64_t n) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    x[i].im = -x[i].im;
+}
+
+cudaError_t launch_conj(ome_dtype dt, void* x, int64_t n, cudaStream_t s) {
+  if (n == 0) return cudaSuccess;
+  const int64_t nb = (n + 255) / 256;
+  const int grid = (int)(nb < 2048 ? nb : 2048);
+  if (dt == OME_C32) {
+    k_conj<cf32><<<grid, 256, 0, s>>>((cf32*)x, n);
+  } else if (dt == OME_C64) {
+    k_conj<cf64><<<grid, 256, 0, s>>>((cf64*)x, n);
+  } else {
+    return cudaSuccess;
+  }
+  count_launch();
+  return cudaGetLastError();
+}
+
+template <class A>
+__global__ void __launch_bounds__(256) k_fill_one(typename A::T* x, int64_t n) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    x[i] = A::one();
+}
+
+cudaError_t launch_fill_one(ome_dtype dt, void* x, int64_t n, cudaStream_t s) {
+  if (n == 0) return cudaSuccess;
+  const int64_t nb = (n + 255) / 256;
+  const int grid = (int)(nb < 2048 ? nb : 2048);
+  cudaError_t e = cudaErrorInvalidValue;
+  OME_DISPATCH(dt, ALG, k_fill_one<ALG><<<grid, 256, 0, s>>>((typename ALG::T*)x, n); count_launch(); e = cudaGetLastError());
+  return e;
+}
+
+}  // namespace ome

@@ -1,0 +1,54 @@
+// Launchers of libomeb200's kernels (host side).  Each returns the launch's
+// cudaError_t; the argument blocks are defined in common.cuh.
+#pragma once
+#include "common.cuh"
+
+namespace ome {
+
+// Global count of kernel launches issued by the library.
+unsigned long long launch_counter();
+void count_launch(int n = 1);
+
+enum LoopMode { LOOP_THREAD = 0, LOOP_BLOCK = 1 };
+
+// Generic sum-product (loop_einsum): mode LOOP_THREAD = one thread per output
+// element; LOOP_BLOCK = one block per output (a.nsplit == 1) or nsplit blocks
+// per output writing partials to a.partial, finished by launch_loop_finish.
+cudaError_t launch_loop(ome_dtype dt, const LoopArgs& a, LoopMode mode, int grid, int block,
+                        cudaStream_t s);
+cudaError_t launch_loop_finish(ome_dtype dt, const LoopArgs& a, cudaStream_t s);
+
+// Permute / broadcast / identity copy with the αβ epilogue.
+cudaError_t launch_perm(ome_dtype dt, const PermArgs& a, int num_sms, cudaStream_t s);
+
+// y <- sy*y (or the algebra's zero when sy_zero) over a strided view.
+cudaError_t launch_scale(ome_dtype dt, void* y, int nd, const int64_t* ext, const int64_t* str,
+                         const Scalar& sy, int sy_zero, int num_sms, cudaStream_t s);
+
+// CUDA-core strided batched GEMM over any algebra.
+cudaError_t launch_gemm_simt(ome_dtype dt, const GemmArgs& g, cudaStream_t s);
+
+// acc[i] (double / double2) += (double) src[i] for n elements, contiguous;
+// FP64 cross-slice accumulation.  dt is the element type of src.
+cudaError_t launch_acc64(ome_dtype dt, void* acc, const void* src, int64_t n, cudaStream_t s);
+// y <- sx*(T)acc + sy*y over n contiguous elements (final slice write-back).
+cudaError_t launch_acc64_store(ome_dtype dt, void* y, const void* acc, int64_t n, const Scalar& sx,
+                               const Scalar& sy, int sy_zero, cudaStream_t s);
+
+// acc (double / double2, strided view with nd modes) += src (contiguous, same
+// mode order, column-major).
+cudaError_t launch_acc64_strided(ome_dtype dt, void* acc, const void* src, int nd, const int64_t* ext,
+                                 const int64_t* acc_str, cudaStream_t s);
+// x <- conj(x) (complex dtypes) over n contiguous elements.
+cudaError_t launch_conj(ome_dtype dt, void* x, int64_t n, cudaStream_t s);
+// x <- one(T) over n contiguous elements.
+cudaError_t launch_fill_one(ome_dtype dt, void* x, int64_t n, cudaStream_t s);
+
+// Tensor-core FP32 GEMM from BF16x3 split products (tcgen05 + TMEM).
+// Returns cudaErrorNotSupported when the shape/strides are outside the
+// kernel's preconditions (the caller then uses the CUDA-core kernel).
+cudaError_t launch_gemm_bf16x3(const GemmArgs& g, void* workspace, size_t ws_bytes, int num_sms,
+                               cudaStream_t s);
+bool gemm_bf16x3_supported(const GemmArgs& g);
+
+}  // namespace ome

@@ -1,0 +1,315 @@
+"""einsum / einsum! / loop_einsum / einsum_grad / cost_and_gradient on the B200 backend.
+
+Host side of the backend: turns codes and torch tensors into C-ABI calls of
+libomeb200 (include/ome_b200.h).  Mirrors the reference's entry points:
+``einsum`` and ``einsum!`` (src/einsum.jl:24-50), ``loop_einsum`` /
+``loop_einsum!`` (src/loop_einsum.jl:8-32), NestedEinsum/SlicedEinsum
+evaluation (src/einsequence.jl:257-287, src/slicing.jl:104-137),
+``einsum_grad`` (src/autodiff.jl:24-30) and ``cost_and_gradient``
+(src/bp.jl:122-130).  Tensors are torch tensors; CUDA tensors stay on their
+device, host (CPU / NumPy) inputs are copied to the current device and the
+result copied back.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from typing import Any, Dict, List, Sequence, Tuple
+
+import numpy as np
+import torch
+
+from . import _lib
+from ._lib import ArgumentError, check
+from .backends import B200Backend, get_einsum_backend
+from .core import (AbstractEinsum, EinCode, NestedEinsum, SlicedEinsum, get_size_dict)
+
+# ----------------------------------------------------------------------------
+# element types
+# ----------------------------------------------------------------------------
+
+
+class TropicalTensor:
+    """A tensor of TropicalNumbers.jl ``Tropical{T}`` values (max-plus algebra)
+    stored as a float32/float64 torch tensor of their contents."""
+
+    def __init__(self, data):
+        if not isinstance(data, torch.Tensor):
+            data = torch.as_tensor(np.asarray(data))
+        if data.dtype not in (torch.float32, torch.float64):
+            data = data.to(torch.float64)
+        self.data = data
+
+    @property
+    def shape(self):
+        return self.data.shape
+
+    @property
+    def dtype(self):
+        return self.data.dtype
+
+    @property
+    def device(self):
+        return self.data.device
+
+    def cpu(self):
+        return TropicalTensor(self.data.cpu())
+
+    def __repr__(self):
+        return f"TropicalTensor({self.data!r})"
+
+
+_TORCH_TO_OME = {
+    torch.float32: _lib.F32, torch.float64: _lib.F64, torch.complex64: _lib.C32,
+    torch.complex128: _lib.C64, torch.int64: _lib.I64, torch.bool: _lib.BOOL,
+}
+_RANK = {torch.bool: 0, torch.int64: 1, torch.float32: 2, torch.float64: 3}
+
+
+def promote_dtype(dts: Sequence[torch.dtype]) -> torch.dtype:
+    """Julia ``promote_type`` over Bool/Int64/Float32/Float64 and complexes
+    (Int64 with Float32 gives Float32, unlike NumPy)."""
+    cplx = any(d.is_complex for d in dts)
+    real = [torch.float32 if d == torch.complex64 else torch.float64 if d == torch.complex128 else d for d in dts]
+    for d in real:
+        if d not in _RANK:
+            raise _lib.OMEError(f"unsupported element type {d}")
+    r = max(real, key=lambda d: _RANK[d])
+    if cplx:
+        return torch.complex128 if r == torch.float64 else torch.complex64
+    return r
+
+
+def _as_tensor(x):
+    if isinstance(x, (torch.Tensor, TropicalTensor)):
+        return x
+    return torch.as_tensor(np.asarray(x))
+
+
+def _colmajor_strides(shape) -> Tuple[int, ...]:
+    s, out = 1, []
+    for e in shape:
+        out.append(s)
+        s *= int(e)
+    return tuple(out)
+
+
+def _alloc(shape, dtype, device) -> torch.Tensor:
+    """Column-major (Julia-layout) output array."""
+    return torch.empty_strided(tuple(shape), _colmajor_strides(shape), dtype=dtype, device=device)
+
+
+def _f_contig(x: torch.Tensor) -> torch.Tensor:
+    if x.dim() == 0 or tuple(x.stride()) == _colmajor_strides(x.shape) or x.numel() <= 1:
+        return x
+    y = _alloc(x.shape, x.dtype, x.device)
+    y.copy_(x)
+    return y
+
+
+class _Prepared:
+    """Inputs moved to one CUDA device with one element type."""
+
+    def __init__(self, xs: Sequence[Any], out_dtype=None):
+        xs = [_as_tensor(x) for x in xs]
+        self.tropical = any(isinstance(x, TropicalTensor) for x in xs)
+        if self.tropical and not all(isinstance(x, TropicalTensor) for x in xs):
+            raise ArgumentError("cannot mix tropical and ordinary tensors")
+        raw = [x.data if isinstance(x, TropicalTensor) else x for x in xs]
+        self.host = all(not t.is_cuda for t in raw)
+        if self.host:
+            dev = torch.device("cuda", torch.cuda.current_device())
+        else:
+            dev = next(t.device for t in raw if t.is_cuda)
+        self.device = dev
+        self.dtype = out_dtype or promote_dtype([t.dtype for t in raw])
+        ts = []
+        for t in raw:
+            if t.is_conj():
+                t = t.resolve_conj()
+            if t.dtype != self.dtype:
+                t = t.to(device=dev, dtype=self.dtype, non_blocking=True)
+            elif t.device != dev:
+                t = t.to(dev, non_blocking=True)
+            ts.append(t)
+        self.tensors = ts
+        if self.tropical:
+            self.ome = _lib.TROP_F32 if self.dtype == torch.float32 else _lib.TROP_F64
+        else:
+            self.ome = _TORCH_TO_OME[self.dtype]
+
+    def wrap(self, y: torch.Tensor):
+        if self.host:
+            y = y.cpu()
+        return TropicalTensor(y) if self.tropical else y
+
+
+def _scalar_buf(ome: int, v) -> C.Array:
+    """One value of the call's dtype; Python bools are the algebra's one/zero
+    (Julia converts true/false to one(T)/zero(T))."""
+    b = (C.c_ubyte * 16)()
+    if ome in (_lib.TROP_F32, _lib.TROP_F64):
+        val = (0.0 if v else -np.inf) if isinstance(v, (bool, np.bool_)) else float(v)
+        arr = np.array([val], dtype=np.float32 if ome == _lib.TROP_F32 else np.float64)
+    elif ome == _lib.BOOL:
+        arr = np.array([bool(v)], dtype=np.uint8)
+    elif ome == _lib.I64:
+        arr = np.array([int(v)], dtype=np.int64)
+    elif ome == _lib.F32:
+        arr = np.array([float(v)], dtype=np.float32)
+    elif ome == _lib.F64:
+        arr = np.array([float(v)], dtype=np.float64)
+    elif ome == _lib.C32:
+        arr = np.array([complex(v)], dtype=np.complex64)
+    else:
+        arr = np.array([complex(v)], dtype=np.complex128)
+    raw = arr.tobytes()
+    C.memmove(b, raw, len(raw))
+    return b
+
+
+class _LabelMap:
+    def __init__(self):
+        self.ids: Dict[Any, int] = {}
+
+    def __call__(self, l) -> int:
+        if l not in self.ids:
+            self.ids[l] = len(self.ids)
+        return self.ids[l]
+
+
+def _tensor_struct(t: torch.Tensor, labels: Sequence[int], keep: list) -> _lib.Tensor:
+    nd = t.dim()
+    dims = (C.c_int64 * max(nd, 1))(*[int(s) for s in t.shape])
+    strides = (C.c_int64 * max(nd, 1))(*[int(s) for s in t.stride()])
+    labs = (C.c_int32 * max(nd, 1))(*labels)
+    keep.extend([dims, strides, labs])
+    return _lib.Tensor(t.data_ptr(), nd, dims, strides, labs)
+
+
+def _stream(device) -> C.c_void_p:
+    return C.c_void_p(torch.cuda.current_stream(device).cuda_stream)
+
+
+def _require_b200():
+    be = get_einsum_backend()
+    if not isinstance(be, B200Backend):
+        raise _lib.OMEError(f"backend {type(be).__name__} is not provided by this package; "
+                            "select B200Backend() with set_einsum_backend")
+    return be
+
+
+def _run_eincode(ixs, iy, p: _Prepared, y: torch.Tensor, sx, sy, loop_only=False, prec=None):
+    be = _require_b200()
+    lm = _LabelMap()
+    keep: list = []
+    xs = (_lib.Tensor * len(ixs))()
+    for i, (ix, t) in enumerate(zip(ixs, p.tensors)):
+        if len(ix) != t.dim():
+            raise ArgumentError(f"indices {tuple(ix)} invalid for tensor with ndims = {t.dim()}")
+        xs[i] = _tensor_struct(t, [lm(l) for l in ix], keep)
+    yt = _tensor_struct(y, [lm(l) for l in iy], keep)
+    sxb, syb = _scalar_buf(p.ome, sx), _scalar_buf(p.ome, sy)
+    ctx = _lib.context(y.device.index if y.device.index is not None else torch.cuda.current_device())
+    lib = _lib.load()
+    prec = be.prec if prec is None else prec
+    with torch.cuda.device(y.device):
+        if loop_only:
+            rc = lib.ome_loop_einsum(ctx.handle, _stream(y.device), p.ome, len(ixs), xs, C.byref(yt), sxb, syb)
+        else:
+            rc = lib.ome_einsum(ctx.handle, _stream(y.device), p.ome, len(ixs), xs, C.byref(yt), sxb, syb, prec)
+    check(rc)
+    return y
+
+
+# ----------------------------------------------------------------------------
+# public API
+# ----------------------------------------------------------------------------
+
+
+def get_output_array(xs, shape, fillzero=False):
+    """``get_output_array`` (src/loop_einsum.jl:48-61; ext/CUDAExt.jl:34-47)."""
+    p = _Prepared(xs)
+    y = _alloc(shape, p.dtype, p.device)
+    if fillzero:
+        y.fill_(-np.inf if p.tropical else 0)
+    return p.wrap(y)
+
+
+def einsum(code: AbstractEinsum, xs: Sequence[Any], size_dict: Dict[Any, int] | None = None, **kw):
+    """``einsum(code, xs, size_dict)``: a new output array (src/einsum.jl:24-27)."""
+    _require_b200()
+    if isinstance(code, (NestedEinsum, SlicedEinsum)):
+        from .plan import run_tree
+        return run_tree(code, xs, size_dict)
+    if size_dict is None:
+        size_dict = get_size_dict(code.getixs(), xs)
+    p = _Prepared(xs)
+    for l in code.iy:
+        if l not in size_dict:
+            raise ArgumentError(f"output label {l} has no size; pass size_info")
+    y = _alloc([size_dict[l] for l in code.iy], p.dtype, p.device)
+    _run_eincode(code.ixs, code.iy, p, y, True, False, **kw)
+    return p.wrap(y)
+
+
+def einsum_(code: AbstractEinsum, xs: Sequence[Any], y, sx=True, sy=False, size_dict=None, **kw):
+    """``einsum!(code, xs, y, sx, sy, size_dict)``: y <- sy*y + sx*code(xs), in place
+    (src/einsum.jl:28-50).  ``y`` must be a CUDA tensor (or TropicalTensor)."""
+    _require_b200()
+    yt = y.data if isinstance(y, TropicalTensor) else y
+    if not yt.is_cuda:
+        raise ArgumentError("einsum_ needs a CUDA output tensor")
+    if isinstance(code, (NestedEinsum, SlicedEinsum)):
+        from .plan import run_tree
+        return run_tree(code, xs, size_dict, y=y, sx=sx, sy=sy)
+    if size_dict is None:
+        size_dict = get_size_dict(code.getixs(), xs)
+    p = _Prepared(xs, out_dtype=yt.dtype)
+    _run_eincode(code.ixs, code.iy, p, yt, sx, sy, **kw)
+    return y
+
+
+def loop_einsum(code: EinCode, xs, size_dict=None):
+    """``loop_einsum`` (src/loop_einsum.jl:8-12): the generic index kernel."""
+    _require_b200()
+    if size_dict is None:
+        size_dict = get_size_dict(code.getixs(), xs)
+    p = _Prepared(xs)
+    y = _alloc([size_dict[l] for l in code.iy], p.dtype, p.device)
+    _run_eincode(code.ixs, code.iy, p, y, True, False, loop_only=True)
+    return p.wrap(y)
+
+
+def loop_einsum_(ixs, iy, xs, y, sx, sy, size_dict=None):
+    """``loop_einsum!`` (src/loop_einsum.jl:21-32)."""
+    yt = y.data if isinstance(y, TropicalTensor) else y
+    p = _Prepared(xs, out_dtype=yt.dtype)
+    _run_eincode([tuple(ix) for ix in ixs], tuple(iy), p, yt, sx, sy, loop_only=True)
+    return y
+
+
+def einsum_grad(ixs, xs, iy, size_dict, dy, i):
+    """``einsum_grad`` (src/autodiff.jl:24-30): the gradient of ``einsum`` w.r.t.
+    input ``i`` (0-based): contract conj(dy) in place of input i into ixs[i],
+    then conjugate."""
+    nixs = [tuple(ix) for ix in ixs]
+    nixs[i] = tuple(iy)
+    nxs = list(xs)
+    dyt = _as_tensor(dy)
+    if isinstance(dyt, torch.Tensor) and dyt.is_complex():
+        dyt = torch.conj_physical(dyt)
+    nxs[i] = dyt
+    y = einsum(EinCode(nixs, ixs[i]), nxs, size_dict)
+    if isinstance(y, torch.Tensor) and y.is_complex():
+        y = torch.conj_physical(y)
+        xi = _as_tensor(xs[i])
+        if isinstance(xi, torch.Tensor) and not xi.is_complex():
+            y = y.real.contiguous()
+    return y
+
+
+def cost_and_gradient(code, xs, dy=None):
+    """``cost_and_gradient`` (src/bp.jl:122-130) on the device: returns
+    (cost, [gradient of each input])."""
+    from .plan import tree_gradient
+    return tree_gradient(code, xs, dy)

@@ -1,0 +1,180 @@
+"""GPU parity: libomeb200 (through the C ABI via the package) against the oracle
+on seeded inputs.  Case lists follow the reference's own tests
+(test/cueinsum.jl, test/einsum.jl, test/binaryrules.jl, test/unaryrules.jl).
+"""
+import itertools
+import zlib
+
+import numpy as np
+import pytest
+import torch
+
+import ome_oracle as O
+import omeinsum_b200 as ome
+from helpers import DTYPES, assert_match, gen, oracle, parse, to_dev, to_np
+
+pytestmark = pytest.mark.gpu
+
+UNARY = ["ij->", "ij->j", "ii->", "ii->i", "ijk->kij", "a->aaaa", "ac->acc", "->ii", "i->ik", "->ik",
+         "illljkk->kijjcc", "ijkl->ijkl", "ijk->ki", "ijk->", "iijj->", "ij->ji", "ijk->jik"]
+BINARY = [",->", "i,->i", "j,j->", ",k->k", "j,jk->k", "j,kj->k", "ij,j->i", "ji,j->i", "i,k->ik", "i,k->ki"]
+for X1, X2, X3 in itertools.product(["ij", "ji"], ["jk", "kj"], ["ik", "ki"]):
+    BINARY.append(f"{X1},{X2}->{X3}")
+BINARY += [c.replace(",", "l,").replace("->", "l->") + "l" for c in list(BINARY)]
+COMPOSITE = ["abb,bc->ac", "ab,bc->acc", "ab,bce->ac", "ab,bc->ace", "bal,bcl->lcae", "bal,bcl->ca",
+             "bal,bc->lca", "ddebal,bcf->lcac", "c,c->cc", "c,cc->c", "cc,c->cc", "cc,cc->cc", "cc,cb->bc",
+             "cb,bc->cc", "ac,cc->ac", "ijk,jkl->il", "ij,ik,il->jkl", "ij,jk,kl->il", "ij,ij,ij->ij"]
+
+
+def run_case(code, dt, D=2, seed=0, sx=True, sy=False, size_info=None):
+    rng = np.random.default_rng(seed)
+    ixs, iy = parse(code)
+    sd = {l: D for l in "abcdefghijklmnopqrstuvwxyz"}
+    if size_info:
+        sd.update(size_info)
+    xs = [gen(rng, [sd[l] for l in ix], dt) for ix in ixs]
+    want = oracle(ixs, iy, xs, sd, dt)
+    got = ome.einsum(ome.EinCode(ixs, iy), [to_dev(x, dt) for x in xs], sd)
+    assert_match(to_np(got), want, dt)
+    if dt in ("f32", "c64"):
+        assert_match(to_np(got), oracle(ixs, iy, xs, sd, dt, wide=True), dt)
+
+
+@pytest.mark.parametrize("dt", DTYPES)
+@pytest.mark.parametrize("code", UNARY)
+def test_unary_rules(code, dt):
+    run_case(code, dt, D=3, seed=zlib.crc32(code.encode()) % 1000)
+
+
+@pytest.mark.parametrize("dt", DTYPES)
+@pytest.mark.parametrize("code", BINARY)
+def test_binary_rules(code, dt):
+    run_case(code, dt, D=3, seed=zlib.crc32(code.encode()) % 1000)
+
+
+@pytest.mark.parametrize("dt", DTYPES)
+@pytest.mark.parametrize("code", COMPOSITE)
+def test_composite_rules(code, dt):
+    run_case(code, dt, D=3, seed=zlib.crc32(code.encode()) % 1000)
+
+
+@pytest.mark.parametrize("dt", ["f64", "c128", "i64", "trop"])
+def test_nary_reference_cases(dt):
+    # test/cueinsum.jl:45-49, 62-78 (D = 2 networks)
+    run_case("npu,por,dom,lmn->urdl", dt, D=2)
+    run_case("abewcd,bfixgh,ajeycd,jfizgh->wxyz", dt, D=2)
+
+
+@pytest.mark.parametrize("dt", DTYPES)
+@pytest.mark.parametrize("sxy", [(5, 3), (5, 1), (2, 0), (0, 3)])
+def test_alpha_beta(dt, sxy):
+    # test/einsum.jl:55-66 and test/cueinsum.jl:15-28: y <- sy*y + sx*f(xs)
+    if dt == "bool":
+        sxy = (bool(sxy[0]), bool(sxy[1]))
+    if dt == "trop":
+        sxy = (float(sxy[0]), float(sxy[1]) if sxy[1] else -np.inf)
+    sx, sy = sxy
+    rng = np.random.default_rng(7)
+    for code in ["ij,jk->ik", "ijl,jkl->ikl", "abb,bc->acc", "ij->ji", "ij->", "ij,ik,il->jkl", "i->ii"]:
+        ixs, iy = parse(code)
+        sd = {l: 3 for l in "abcijkl"}
+        xs = [gen(rng, [sd[l] for l in ix], dt) for ix in ixs]
+        y0 = gen(rng, [sd[l] for l in iy], dt)
+        yd = to_dev(y0, dt)
+        ome.einsum_(ome.EinCode(ixs, iy), [to_dev(x, dt) for x in xs], yd, sx, sy, sd)
+        want = np.array(y0, order="F")
+        O.einsum_(ixs, iy, xs, want, sx, sy, sd, O.TROPICAL if dt == "trop" else None)
+        assert_match(to_np(yd), want, dt)
+
+
+def test_size_info_broadcast_identity():
+    # test/einsum.jl:191-194: ein"->ii"(1; size_info = i=>5) == I(5)
+    got = ome.ein("->ii")(torch.ones((), dtype=torch.int64, device="cuda"), size_info={"i": 5})
+    assert torch.equal(got.cpu(), torch.eye(5, dtype=torch.int64))
+    r = ome.ein(",->")(torch.tensor(3, device="cuda"), torch.tensor(4, device="cuda"))
+    assert r.dtype == torch.int64 and int(r) == 12
+
+
+def test_high_rank_permute():
+    # test/cueinsum.jl:164-167: rank-18 permutedims
+    rng = np.random.default_rng(3)
+    shape = [4] + [int(v) for v in rng.integers(1, 4, 17)]
+    x = rng.standard_normal(shape)
+    labels = [chr(ord("a") + i) for i in range(18)]
+    code = ome.EinCode([labels], labels[::-1])
+    got = to_np(ome.einsum(code, [to_dev(x, "f64")]))
+    assert np.array_equal(got, np.transpose(x, list(range(17, -1, -1))))
+
+
+@pytest.mark.parametrize("dt", ["f32", "f64", "c64", "i64", "trop", "bool"])
+@pytest.mark.parametrize("code,sizes", [
+    ("ij,jk->ik", dict(i=200, j=300, k=250)),
+    ("ji,jk->ki", dict(i=130, j=70, k=90)),
+    ("ij,kj->ik", dict(i=64, j=200, k=96)),
+    ("bij,bjk->bik", dict(b=40, i=33, j=65, k=40)),
+    ("abcd,cdef->abef", dict(a=12, b=12, c=12, d=12, e=12, f=12)),
+    ("ijk,jkl->il", dict(i=40, j=40, k=40, l=40)),
+    ("ijl,jkl->kil", dict(i=48, j=64, k=80, l=3)),
+])
+def test_gemm_shapes(code, sizes, dt):
+    """GEMM-shaped contractions (strided GEMM / BF16x3 tensor-core path)."""
+    rng = np.random.default_rng(11)
+    ixs, iy = parse(code)
+    xs = [gen(rng, [sizes[l] for l in ix], dt) for ix in ixs]
+    got = to_np(ome.einsum(ome.EinCode(ixs, iy), [to_dev(x, dt) for x in xs], sizes))
+    want = oracle(ixs, iy, xs, sizes, dt)
+    assert_match(got, want, dt)
+    if dt in ("f32", "c64"):
+        assert_match(got, oracle(ixs, iy, xs, sizes, dt, wide=True), dt)
+
+
+def test_plain_fp32_path_matches():
+    rng = np.random.default_rng(5)
+    a, b = rng.standard_normal((200, 300)).astype(np.float32), rng.standard_normal((300, 100)).astype(np.float32)
+    ome.set_einsum_backend(ome.B200Backend(prec=1))
+    try:
+        got = to_np(ome.ein("ij,jk->ik")(to_dev(a, "f32"), to_dev(b, "f32")))
+    finally:
+        ome.set_einsum_backend(ome.B200Backend())
+    assert_match(got, a.astype(np.float64) @ b.astype(np.float64), "f32")
+
+
+def test_loop_einsum_entry():
+    # test/cueinsum.jl:15-28: loop_einsum! with sx, sy and a duplicated output label
+    rng = np.random.default_rng(2)
+    a = rng.standard_normal((3, 3))
+    ad = to_dev(a, "f64")
+    y = torch.ones((3, 3, 3), dtype=torch.float64, device="cuda")
+    ome.loop_einsum_([(1, 2), (2, 3)], (1, 3, 3), [ad, ad], y, 4.0, 2.0)
+    out = 2 * np.ones((3, 3, 3))
+    res = 4.0 * a @ a
+    for k in range(3):
+        out[:, k, k] += res[:, k]
+    assert np.allclose(to_np(y), out)
+    assert np.allclose(to_np(ome.loop_einsum(ome.ein("ij,jk->ik"), [ad, ad])), a @ a)
+
+
+def test_errors_from_library():
+    a = torch.zeros(3, 3, device="cuda")
+    b = torch.zeros(4, 4, device="cuda")
+    with pytest.raises(ome.DimensionMismatch):
+        ome.einsum(ome.EinCode([(1, 2), (2, 3)], (1, 3)), [a, b], {1: 3, 2: 3, 3: 3})
+    with pytest.raises(ome.ArgumentError):
+        ome.einsum(ome.EinCode([(1, 2, 3), (2, 3)], (1, 3)), [a, a], {1: 3, 2: 3, 3: 3})
+
+
+def test_host_buffers_round_trip():
+    rng = np.random.default_rng(4)
+    a, b = rng.standard_normal((20, 30)), rng.standard_normal((30, 10))
+    got = ome.ein("ij,jk->ik")(torch.from_numpy(a), torch.from_numpy(b))
+    assert not got.is_cuda and np.allclose(got.numpy(), a @ b)
+
+
+def test_empty_extents():
+    # test/einsum.jl:306-309 (issue 136)
+    got = ome.EinCode([(1, 2, 3), (2,)], (1, 3))(torch.ones(2, 2, 1, device="cuda"), torch.ones(2, device="cuda"))
+    assert torch.equal(got.cpu(), torch.tensor([[2.0], [2.0]]))
+    got = ome.EinCode([(1, 2, 3), (2,)], (1, 3))(torch.ones(2, 2, 0, device="cuda"), torch.ones(2, device="cuda"))
+    assert tuple(got.shape) == (2, 0)
+    got = ome.ein("ij,jk->ik")(torch.ones(3, 0, device="cuda"), torch.ones(0, 4, device="cuda"))
+    assert torch.equal(got.cpu(), torch.zeros(3, 4))
