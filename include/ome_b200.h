@@ -91,6 +91,13 @@ OME_API int ome_version(void);
  * threads); lets a caller count device launches in a timed region. */
 OME_API unsigned long long ome_launch_count(void);
 
+/* Synchronise `stream` (a cudaStream_t, NULL = legacy default stream), then
+ * report whether any kernel of this library gave up a bounded device-side
+ * wait since the last call: OME_TIMEOUT if so (the flag is cleared), else
+ * OME_OK.  Kernels never spin unboundedly; a wait that gives up marks its
+ * result invalid through this flag instead of trapping. */
+OME_API int ome_device_status(void* stream);
+
 /* Message of the last failed call on this host thread ("" if none). */
 OME_API const char* ome_last_error(void);
 

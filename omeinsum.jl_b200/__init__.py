@@ -20,7 +20,7 @@ Public API (names follow OMEinsum.jl; ``!`` becomes a trailing ``_``):
 
 Every contraction runs in libomeb200.so; there is no CPU fallback.
 """
-from ._lib import ArgumentError, DimensionMismatch, OMEError, load as load_library
+from ._lib import ArgumentError, DimensionMismatch, OMEError, device_status, load as load_library
 from .backends import (B200Backend, CuTensorBackend, DefaultBackend, EinsumBackend, get_einsum_backend,
                        set_einsum_backend)
 from .core import (AbstractEinsum, DynamicEinCode, DynamicNestedEinsum, EinCode, NestedEinsum, SlicedEinsum,

@@ -20,7 +20,7 @@ F32, F64, C32, C64, I64, BOOL, TROP_F32, TROP_F64 = range(8)
 PREC_AUTO, PREC_FP32, PREC_BF16X3 = range(3)
 
 EXPORTS = [
-    "ome_version", "ome_launch_count", "ome_last_error", "ome_ctx_create", "ome_ctx_destroy", "ome_ctx_workspace_bytes",
+    "ome_version", "ome_launch_count", "ome_device_status", "ome_last_error", "ome_ctx_create", "ome_ctx_destroy", "ome_ctx_workspace_bytes",
     "ome_einsum", "ome_loop_einsum", "ome_plan_create", "ome_plan_destroy", "ome_plan_peak_bytes",
     "ome_plan_execute", "ome_plan_gradient",
 ]
@@ -71,6 +71,7 @@ def load() -> C.CDLL:
         lib.ome_version.restype = C.c_int
         lib.ome_launch_count.restype = C.c_ulonglong
         lib.ome_last_error.restype = C.c_char_p
+        lib.ome_device_status.argtypes = [P]
         lib.ome_ctx_create.argtypes = [C.c_int, C.c_size_t, C.POINTER(P)]
         lib.ome_ctx_destroy.argtypes = [P]
         lib.ome_ctx_workspace_bytes.argtypes = [P, C.POINTER(C.c_size_t)]
@@ -101,6 +102,11 @@ def check(rc: int) -> None:
     if rc == OUT_OF_MEMORY:
         raise MemoryError(msg)
     raise OMEError(f"[status {rc}] {msg}")
+
+
+def device_status(stream=None) -> None:
+    """Synchronise and raise OMEError if a bounded device-side wait gave up."""
+    check(load().ome_device_status(stream))
 
 
 class Context:

@@ -538,6 +538,13 @@ int ome_version(void) { return 1; }
 
 unsigned long long ome_launch_count(void) { return ome::launch_counter(); }
 
+int ome_device_status(void* stream) {
+  const int r = ome::device_status(static_cast<cudaStream_t>(stream));
+  if (r < 0) return cuda_err((cudaError_t)(-r), "device status");
+  if (r > 0) return set_err(OME_TIMEOUT, "a device-side wait gave up (bounded wait expired)");
+  return OME_OK;
+}
+
 const char* ome_last_error(void) { return g_err.c_str(); }
 
 int ome_ctx_create(int device, size_t workspace_bytes, ome_ctx** out) {

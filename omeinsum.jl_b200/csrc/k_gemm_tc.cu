@@ -1,6 +1,452 @@
-// placeholder: replaced by the tcgen05 BF16x3 kernel
+// Tensor-core FP32 contraction from BF16x3 split products (sm_100a tcgen05).
+//
+// Replaces the GEMM at the heart of OMEinsum's binary path
+// (src/einsum.jl:104-124 -> src/binaryrules.jl mul!/_batched_gemm!, on GPU
+// CUBLAS gemm / gemm_strided_batched, ext/CUDAExt.jl:115-117,156-178).
+//
+// Design:
+//  * operands are read in place from the input tensors through per-group
+//    mode strides (the permutation of simplifyto, src/einsum.jl:127-134, is
+//    absorbed in the addressing; nothing is written back to HBM);
+//  * 8 converter warps load FP32 from global memory (coalesced along the
+//    operand's contiguous mode), split each value x into hi = bf16(x) and
+//    lo = bf16(x - hi) and store both into shared memory in the UMMA K-major
+//    no-swizzle canonical layout (8-row x 16-byte core matrices);
+//  * one elected thread of a ninth warp issues, per K=16 step, three
+//    tcgen05.mma kind::f16 (hi*hi + hi*lo + lo*hi) accumulating in FP32 in
+//    tensor memory; tcgen05.commit releases each shared-memory stage;
+//  * the converter warps then read the 128x128 FP32 accumulator from TMEM
+//    (tcgen05.ld) and apply the y <- sy*y + sx*f epilogue through the
+//    output's mode strides, or write a split-K partial that a second kernel
+//    sums in a fixed order (deterministic);
+//  * every mbarrier wait is bounded (about 2 s of %globaltimer); on expiry the
+//    kernel records g_ome_timeout, stops waiting and frees its TMEM.
+#include <cuda_bf16.h>
+#include <string.h>
 #include "kernels.h"
+
 namespace ome {
-bool gemm_bf16x3_supported(const GemmArgs&) { return false; }
-cudaError_t launch_gemm_bf16x3(const GemmArgs&, void*, size_t, int, cudaStream_t) { return cudaErrorNotSupported; }
+
+__device__ int g_ome_timeout = 0;
+
+namespace tc {
+constexpr int BM = 128, BN = 128, BK = 32;
+constexpr int STAGES = 3;
+constexpr int NCONV = 256;                 // converter + epilogue threads (8 warps)
+constexpr int NTHREADS = NCONV + 32;       // + one MMA-issue warp
+constexpr int TILE_BYTES = BM * BK * 2;    // one bf16 operand tile (hi or lo): 8 KB
+constexpr int STAGE_BYTES = 4 * TILE_BYTES;  // A hi, A lo, B hi, B lo
+constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 256;
+constexpr int TMEM_COLS = 128;
+constexpr unsigned long long WAIT_NS = 2000000000ull;
+// kind::f16, BF16 x BF16 -> F32, K-major A and B, M = 128, N = 128
+constexpr uint32_t IDESC = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(BN >> 3) << 17) |
+                           ((uint32_t)(BM >> 4) << 24);
+}  // namespace tc
+
+struct TcArgs {
+  GemmArgs g;
+  int S;               // K splits
+  int64_t kchunk;      // K elements per split (multiple of BK)
+  float* partial;      // S > 1: [S][L][N][M] partial sums
+  int a_kfast, b_kfast;  // the operand's first K mode is contiguous and a multiple of 8 long
+};
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
 }
+__device__ __forceinline__ uint64_t gtimer() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}\n"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// Bounded wait: false once the block has given up (abort flag set by any thread).
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, volatile int* abort_flag) {
+  if (mbar_try_wait(bar, parity)) return true;
+  const uint64_t t0 = gtimer();
+  while (true) {
+#pragma unroll 1
+    for (int i = 0; i < 32; ++i)
+      if (mbar_try_wait(bar, parity)) return true;
+    if (*abort_flag) return false;
+    if (gtimer() - t0 > tc::WAIT_NS) {
+      *abort_flag = 1;
+      atomicExch(&g_ome_timeout, 1);
+      return false;
+    }
+  }
+}
+__device__ __forceinline__ void fence_proxy_async() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+__device__ __forceinline__ void tc_fence_before() {
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void tc_fence_after() {
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr) {
+  // K-major, no swizzle: LBO = 128 B between K-adjacent core matrices,
+  // SBO = 512 B between 8-row groups (4 K-chunks of a BK=32 row group).
+  return (uint64_t)((saddr >> 4) & 0x3FFF) | ((uint64_t)(128 >> 4) << 16) | ((uint64_t)(512 >> 4) << 32) |
+         (1ull << 46);
+}
+__device__ __forceinline__ void umma_bf16(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t acc) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(d_tmem),
+      "l"(a), "l"(b), "r"(tc::IDESC), "r"(acc));
+}
+__device__ __forceinline__ void umma_commit(uint64_t* bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                   smem_u32(bar))
+               : "memory");
+}
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&r)[32]) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+      "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+      "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
+        "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
+        "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
+__device__ __forceinline__ int64_t goff(int64_t i, int n, const int64_t* ext, const int64_t* str) {
+  if (n == 1) return i * str[0];
+  return mode_offset(i, n, ext, str);
+}
+
+// hi = bf16(x), lo = bf16(x - hi) for 8 values -> 16 B each.
+__device__ __forceinline__ void split8(const float (&v)[8], uint4& hi, uint4& lo) {
+  uint32_t h[4], l[4];
+#pragma unroll
+  for (int p = 0; p < 4; ++p) {
+    __nv_bfloat162 hb = __float22bfloat162_rn(make_float2(v[2 * p], v[2 * p + 1]));
+    float2 hf = __bfloat1622float2(hb);
+    float r0 = isfinite(hf.x) ? v[2 * p] - hf.x : 0.f;
+    float r1 = isfinite(hf.y) ? v[2 * p + 1] - hf.y : 0.f;
+    __nv_bfloat162 lb = __float22bfloat162_rn(make_float2(r0, r1));
+    h[p] = *reinterpret_cast<uint32_t*>(&hb);
+    l[p] = *reinterpret_cast<uint32_t*>(&lb);
+  }
+  hi = make_uint4(h[0], h[1], h[2], h[3]);
+  lo = make_uint4(l[0], l[1], l[2], l[3]);
+}
+
+// Load one unit: 8 consecutive k (k0 .. k0+7) of one row.  rowoff < 0: a row
+// beyond the extent (zeros).  kfast: the first K mode is contiguous and a
+// multiple of 8 long, so the unit is 8 consecutive floats.
+__device__ __forceinline__ void load_unit(const float* __restrict__ base, int64_t rowoff, int64_t k0, int64_t kend,
+                                          int kfast, int nk, const int64_t* kext, const int64_t* kstr,
+                                          float (&v)[8]) {
+  if (rowoff < 0) {
+#pragma unroll
+    for (int i = 0; i < 8; ++i) v[i] = 0.f;
+    return;
+  }
+  if (kfast && k0 + 8 <= kend) {
+    const float* p = base + rowoff + goff(k0, nk, kext, kstr);
+    if ((reinterpret_cast<uintptr_t>(p) & 15) == 0) {
+      const float4 a = __ldg(reinterpret_cast<const float4*>(p));
+      const float4 b = __ldg(reinterpret_cast<const float4*>(p) + 1);
+      v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w;
+      v[4] = b.x; v[5] = b.y; v[6] = b.z; v[7] = b.w;
+    } else {
+#pragma unroll
+      for (int i = 0; i < 8; ++i) v[i] = __ldg(p + i);
+    }
+    return;
+  }
+#pragma unroll
+  for (int i = 0; i < 8; ++i) {
+    const int64_t k = k0 + i;
+    v[i] = k < kend ? __ldg(base + rowoff + goff(k, nk, kext, kstr)) : 0.f;
+  }
+}
+
+__global__ void __launch_bounds__(tc::NTHREADS, 2) k_gemm_bf16x3(const __grid_constant__ TcArgs t) {
+  using namespace tc;
+  extern __shared__ __align__(1024) unsigned char smem[];
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem + STAGES * STAGE_BYTES);
+  uint64_t* empty = full + STAGES;
+  uint64_t* done = empty + STAGES;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(done + 1);
+  volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
+
+  const GemmArgs& g = t.g;
+  const int tid = threadIdx.x;
+  const int warp = tid >> 5, lane = tid & 31;
+  const int64_t m0 = (int64_t)blockIdx.x * BM, n0 = (int64_t)blockIdx.y * BN;
+  const int64_t z = blockIdx.z;
+  const int64_t l = z / t.S;
+  const int64_t split = z - l * t.S;
+  const int64_t kbeg = split * t.kchunk;
+  const int64_t kend = min(g.K, kbeg + t.kchunk);
+  const int nkt = (int)((kend - kbeg + BK - 1) / BK);
+
+  if (tid == 0) {
+    for (int s = 0; s < STAGES; ++s) {
+      mbar_init(&full[s], NCONV);
+      mbar_init(&empty[s], 1);
+    }
+    mbar_init(done, 1);
+    *abort_flag = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == NCONV / 32) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                 "r"(TMEM_COLS)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tmem_slot;
+
+  const float* Ap = static_cast<const float*>(g.A);
+  const float* Bp = static_cast<const float*>(g.B);
+  const int64_t la = mode_offset(l, g.nl, g.l_ext, g.l_sa);
+  const int64_t lb = mode_offset(l, g.nl, g.l_ext, g.l_sb);
+
+  if (warp < NCONV / 32) {
+    // ---------------- converters ----------------
+    // unit u in {0,1} of each operand: (row, kchunk) of the 128 x 32 tile
+    int arow[2], akc[2], brow[2], bkc[2];
+    if (t.a_kfast) {
+      arow[0] = tid >> 2; arow[1] = (tid >> 2) + 64; akc[0] = akc[1] = tid & 3;
+    } else {
+      arow[0] = arow[1] = tid & 127; akc[0] = (tid >> 7) * 2; akc[1] = akc[0] + 1;
+    }
+    if (t.b_kfast) {
+      brow[0] = tid >> 2; brow[1] = (tid >> 2) + 64; bkc[0] = bkc[1] = tid & 3;
+    } else {
+      brow[0] = brow[1] = tid & 127; bkc[0] = (tid >> 7) * 2; bkc[1] = bkc[0] + 1;
+    }
+    int64_t aoff[2], boff[2];
+#pragma unroll
+    for (int u = 0; u < 2; ++u) {
+      const int64_t m = m0 + arow[u], n = n0 + brow[u];
+      aoff[u] = m < g.M ? la + goff(m, g.nm, g.m_ext, g.m_sa) : -1;
+      boff[u] = n < g.N ? lb + goff(n, g.nn, g.n_ext, g.n_sb) : -1;
+    }
+    // shared-memory byte offsets of each unit inside an operand tile
+    uint32_t aso[2], bso[2];
+#pragma unroll
+    for (int u = 0; u < 2; ++u) {
+      aso[u] = (uint32_t)((((arow[u] >> 3) * 4 + akc[u]) * 8 + (arow[u] & 7)) * 16);
+      bso[u] = (uint32_t)((((brow[u] >> 3) * 4 + bkc[u]) * 8 + (brow[u] & 7)) * 16);
+    }
+    float va[2][8], vb[2][8];
+    auto load_stage = [&](int kt) {
+      const int64_t kb = kbeg + (int64_t)kt * BK;
+#pragma unroll
+      for (int u = 0; u < 2; ++u) {
+        load_unit(Ap, aoff[u], kb + akc[u] * 8, kend, t.a_kfast, g.nk, g.k_ext, g.k_sa, va[u]);
+        load_unit(Bp, boff[u], kb + bkc[u] * 8, kend, t.b_kfast, g.nk, g.k_ext, g.k_sb, vb[u]);
+      }
+    };
+    if (nkt > 0) load_stage(0);
+    for (int kt = 0; kt < nkt; ++kt) {
+      float ca[2][8], cb[2][8];
+#pragma unroll
+      for (int u = 0; u < 2; ++u)
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+          ca[u][i] = va[u][i];
+          cb[u][i] = vb[u][i];
+        }
+      if (kt + 1 < nkt) load_stage(kt + 1);  // prefetch the next stage into registers
+      const int s = kt % STAGES;
+      if (kt >= STAGES) mbar_wait(&empty[s], (uint32_t)((kt / STAGES - 1) & 1), abort_flag);
+      unsigned char* st = smem + s * STAGE_BYTES;
+#pragma unroll
+      for (int u = 0; u < 2; ++u) {
+        uint4 hi, lo;
+        split8(ca[u], hi, lo);
+        *reinterpret_cast<uint4*>(st + aso[u]) = hi;
+        *reinterpret_cast<uint4*>(st + TILE_BYTES + aso[u]) = lo;
+        split8(cb[u], hi, lo);
+        *reinterpret_cast<uint4*>(st + 2 * TILE_BYTES + bso[u]) = hi;
+        *reinterpret_cast<uint4*>(st + 3 * TILE_BYTES + bso[u]) = lo;
+      }
+      fence_proxy_async();
+      mbar_arrive(&full[s]);
+    }
+    // ---------------- epilogue ----------------
+    const bool ok = nkt > 0 && mbar_wait(done, 0, abort_flag);
+    tc_fence_after();
+    const int q = warp & 3, h = warp >> 2;
+    const int64_t m = m0 + 32 * q + lane;
+    const bool mok = m < g.M;
+    const int64_t lc = mode_offset(l, g.nl, g.l_ext, g.l_sc);
+    const int64_t cm = mok ? goff(m, g.nm, g.m_ext, g.m_sc) : 0;
+    float* Cp = static_cast<float*>(g.C);
+    const float sx = scalar_as<float>(g.sx), sy = scalar_as<float>(g.sy);
+#pragma unroll 1
+    for (int c = 0; c < 2; ++c) {
+      uint32_t r[32];
+      const int col = 64 * h + 32 * c;
+      __syncwarp();
+      tmem_ld32(tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)col, r);
+      if (!ok) {
+#pragma unroll
+        for (int j = 0; j < 32; ++j) r[j] = 0u;
+      }
+      if (!mok) continue;
+#pragma unroll 4
+      for (int j = 0; j < 32; ++j) {
+        const int64_t n = n0 + col + j;
+        if (n >= g.N) break;
+        const float v = __uint_as_float(r[j]);
+        if (t.S > 1) {
+          t.partial[((split * g.L + l) * g.N + n) * g.M + m] = v;
+        } else {
+          float* cp = Cp + lc + cm + goff(n, g.nn, g.n_ext, g.n_sc);
+          float o = g.sx_one ? v : sx * v;
+          if (!g.sy_zero) o = fmaf(sy, *cp, o);
+          *cp = o;
+        }
+      }
+    }
+  } else if (lane == 0) {
+    // ---------------- MMA issue (one thread) ----------------
+    for (int kt = 0; kt < nkt; ++kt) {
+      const int s = kt % STAGES;
+      if (!mbar_wait(&full[s], (uint32_t)((kt / STAGES) & 1), abort_flag)) break;
+      tc_fence_after();
+      const uint32_t sb = smem_u32(smem + s * STAGE_BYTES);
+#pragma unroll
+      for (int kk = 0; kk < 2; ++kk) {
+        const uint32_t off = kk * 256;
+        const uint64_t ah = umma_desc(sb + off), al = umma_desc(sb + TILE_BYTES + off);
+        const uint64_t bh = umma_desc(sb + 2 * TILE_BYTES + off), bl = umma_desc(sb + 3 * TILE_BYTES + off);
+        umma_bf16(tmem, ah, bh, (kt | kk) != 0);
+        umma_bf16(tmem, ah, bl, 1);
+        umma_bf16(tmem, al, bh, 1);
+      }
+      umma_commit(&empty[s]);
+    }
+    umma_commit(done);
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == NCONV / 32) {
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TMEM_COLS) : "memory");
+  }
+}
+
+// Sum the S partials of each output element in split order; αβ epilogue.
+__global__ void __launch_bounds__(256) k_splitk_reduce(const __grid_constant__ TcArgs t) {
+  const GemmArgs& g = t.g;
+  const float sx = scalar_as<float>(g.sx), sy = scalar_as<float>(g.sy);
+  float* Cp = static_cast<float*>(g.C);
+  const int64_t total = g.M * g.N * g.L;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t m = i % g.M;
+    const int64_t r = i / g.M;
+    const int64_t n = r % g.N;
+    const int64_t l = r / g.N;
+    float acc = 0.f;
+    for (int s = 0; s < t.S; ++s) acc += t.partial[((s * g.L + l) * g.N + n) * g.M + m];
+    float* cp = Cp + mode_offset(l, g.nl, g.l_ext, g.l_sc) + goff(m, g.nm, g.m_ext, g.m_sc) +
+                goff(n, g.nn, g.n_ext, g.n_sc);
+    float o = g.sx_one ? acc : sx * acc;
+    if (!g.sy_zero) o = fmaf(sy, *cp, o);
+    *cp = o;
+  }
+}
+
+bool gemm_bf16x3_supported(const GemmArgs& g) {
+  return g.M > 0 && g.N > 0 && g.K > 0 && g.L > 0 && g.M < (1ll << 31) && g.N < (1ll << 31) &&
+         (g.M + tc::BM - 1) / tc::BM <= 0x7fffffff && (g.N + tc::BN - 1) / tc::BN <= 65535;
+}
+
+cudaError_t launch_gemm_bf16x3(const GemmArgs& g, void* workspace, size_t ws_bytes, int num_sms, cudaStream_t s) {
+  using namespace tc;
+  if (!gemm_bf16x3_supported(g)) return cudaErrorNotSupported;
+  static bool attr_set = false;
+  if (!attr_set) {
+    cudaError_t e = cudaFuncSetAttribute(k_gemm_bf16x3, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES);
+    if (e != cudaSuccess) return e;
+    attr_set = true;
+  }
+  TcArgs t;
+  memset(&t, 0, sizeof(t));
+  t.g = g;
+  t.a_kfast = g.k_sa[0] == 1 && g.k_ext[0] % 8 == 0;
+  t.b_kfast = g.k_sb[0] == 1 && g.k_ext[0] % 8 == 0;
+  const int64_t tm = (g.M + BM - 1) / BM, tn = (g.N + BN - 1) / BN;
+  const int64_t tiles = tm * tn * g.L;
+  // split K until the grid covers the SMs twice (two CTAs per SM), keeping
+  // at least 8 k-steps per split
+  int64_t S = 1;
+  const int64_t ksteps = (g.K + BK - 1) / BK;
+  if (tiles < 2 * num_sms) {
+    S = (2 * num_sms + tiles - 1) / tiles;
+    S = std::min<int64_t>(S, std::max<int64_t>(1, ksteps / 8));
+  }
+  int64_t kchunk = ((ksteps + S - 1) / S) * BK;
+  S = (g.K + kchunk - 1) / kchunk;
+  if (S > 1) {
+    const size_t need = (size_t)S * g.L * g.M * g.N * sizeof(float);
+    if (need > ws_bytes || g.L * S > 65535) {
+      S = 1;
+      kchunk = ksteps * BK;
+    } else {
+      t.partial = static_cast<float*>(workspace);
+    }
+  }
+  if (S == 1 && g.L > 65535) return cudaErrorNotSupported;
+  t.S = (int)S;
+  t.kchunk = kchunk;
+  dim3 grid((unsigned)tm, (unsigned)tn, (unsigned)(g.L * S));
+  k_gemm_bf16x3<<<grid, NTHREADS, SMEM_BYTES, s>>>(t);
+  count_launch();
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess || S == 1) return e;
+  const int64_t total = g.M * g.N * g.L;
+  const int64_t nb = (total + 255) / 256;
+  k_splitk_reduce<<<(unsigned)std::min<int64_t>(nb, (int64_t)num_sms * 16), 256, 0, s>>>(t);
+  count_launch();
+  return cudaGetLastError();
+}
+
+int device_status(cudaStream_t s) {
+  cudaError_t e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) return -(int)e;
+  int flag = 0;
+  e = cudaMemcpyFromSymbol(&flag, g_ome_timeout, sizeof(int));
+  if (e != cudaSuccess) return -(int)e;
+  if (flag) {
+    const int zero = 0;
+    cudaMemcpyToSymbol(g_ome_timeout, &zero, sizeof(int));
+  }
+  return flag;
+}
+
+}  // namespace ome

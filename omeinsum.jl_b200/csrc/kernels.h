@@ -51,4 +51,8 @@ cudaError_t launch_gemm_bf16x3(const GemmArgs& g, void* workspace, size_t ws_byt
                                cudaStream_t s);
 bool gemm_bf16x3_supported(const GemmArgs& g);
 
+// Synchronise s and read/clear the device timeout flag: 1 if a bounded wait
+// gave up, 0 if not, -cudaError on failure.
+int device_status(cudaStream_t s);
+
 }  // namespace ome

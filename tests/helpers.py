@@ -38,7 +38,7 @@ def alg_of(dt):
 
 
 def to_dev(a, dt):
-    t = torch.from_numpy(np.asfortranarray(a)).cuda()
+    t = torch.from_numpy(np.array(a, order="F")).cuda()
     return ome.TropicalTensor(t) if dt == "trop" else t
 
 

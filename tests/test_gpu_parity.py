@@ -122,6 +122,7 @@ def test_gemm_shapes(code, sizes, dt):
     ixs, iy = parse(code)
     xs = [gen(rng, [sizes[l] for l in ix], dt) for ix in ixs]
     got = to_np(ome.einsum(ome.EinCode(ixs, iy), [to_dev(x, dt) for x in xs], sizes))
+    ome.device_status()
     want = oracle(ixs, iy, xs, sizes, dt)
     assert_match(got, want, dt)
     if dt in ("f32", "c64"):
