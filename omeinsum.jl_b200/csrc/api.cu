@@ -275,6 +275,33 @@ static int run_loop(ome_ctx* ctx, cudaStream_t s, ome_dtype dt, int nin, const H
   a.nsplit = 1;
 
   const int sms = ctx->num_sms;
+  // one input whose first summed mode is contiguous: row-vectorised reduction
+  if (nin == 1 && (inner.n == 1 || inner.n == 2) && inner.str[1][0] == 1 && inner.ext[0] >= 32 &&
+      n_out < (int64_t)sms * 2048) {
+    const int64_t R = inner.n == 2 ? inner.ext[1] : 1;
+    const size_t es = dtype_size(dt);
+    const int64_t V = (int64_t)(16 / es);
+    bool vec = inner.ext[0] % V == 0 && ((uintptr_t)xu[0].data % 16) == 0;
+    for (int m = 0; m < outer.n && vec; ++m) vec = (outer.str[1][m] * (int64_t)es) % 16 == 0;
+    if (inner.n == 2) vec = vec && (inner.str[1][1] * (int64_t)es) % 16 == 0;
+    int64_t nsplit = 1;
+    const int64_t target = (int64_t)sms * 8;
+    if (n_out < target) nsplit = std::min<int64_t>((target + n_out - 1) / n_out, R);
+    int64_t rchunk = (R + nsplit - 1) / nsplit;
+    nsplit = (R + rchunk - 1) / rchunk;
+    if (nsplit > 1) {
+      a.partial = ws_alloc(ctx, (size_t)(n_out * nsplit) * es);
+      if (!a.partial) {
+        nsplit = 1;
+        rchunk = R;
+      }
+    }
+    a.nsplit = (int)nsplit;
+    const int grid = (int)std::min<int64_t>(n_out * nsplit, (int64_t)sms * 32);
+    OME_CK(cuda_err(launch_reduce_contig(dt, a, vec, rchunk, grid, s), "reduce kernel"));
+    if (nsplit > 1) OME_CK(cuda_err(launch_loop_finish(dt, a, s), "reduce finish"));
+    return OME_OK;
+  }
   const bool thread_mode = n_in <= 16 || n_out >= (int64_t)sms * 512;
   if (thread_mode) {
     const int64_t nb = (n_out + 255) / 256;
@@ -286,7 +313,7 @@ static int run_loop(ome_ctx* ctx, cudaStream_t s, ome_dtype dt, int nin, const H
   const int64_t target = (int64_t)sms * 8;
   if (n_out < target) {
     nsplit = (target + n_out - 1) / n_out;
-    nsplit = std::min<int64_t>(nsplit, std::max<int64_t>(1, n_in / (block * 8)));
+    nsplit = std::min<int64_t>(nsplit, std::max<int64_t>(1, n_in / (block * 2)));
   }
   if (nsplit > 1) {
     a.partial = ws_alloc(ctx, (size_t)(n_out * nsplit) * dtype_size(dt));

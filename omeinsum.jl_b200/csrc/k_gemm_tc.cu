@@ -8,11 +8,12 @@
 //  * operands are read in place from the input tensors through per-group
 //    mode strides (the permutation of simplifyto, src/einsum.jl:127-134, is
 //    absorbed in the addressing; nothing is written back to HBM);
-//  * 8 converter warps load FP32 from global memory (coalesced along the
+//  * 16 converter warps load FP32 from global memory (coalesced along the
 //    operand's contiguous mode), split each value x into hi = bf16(x) and
 //    lo = bf16(x - hi) and store both into shared memory in the UMMA K-major
 //    no-swizzle canonical layout (8-row x 16-byte core matrices);
-//  * one elected thread of a ninth warp issues, per K=16 step, three
+//    with two stages of loads in flight per thread;
+//  * one elected thread of a seventeenth warp issues, per K=16 step, three
 //    tcgen05.mma kind::f16 (hi*hi + hi*lo + lo*hi) accumulating in FP32 in
 //    tensor memory; tcgen05.commit releases each shared-memory stage;
 //  * the converter warps then read the 128x128 FP32 accumulator from TMEM
@@ -31,8 +32,9 @@ __device__ int g_ome_timeout = 0;
 
 namespace tc {
 constexpr int BM = 128, BN = 128, BK = 32;
-constexpr int STAGES = 3;
-constexpr int NCONV = 256;                 // converter + epilogue threads (8 warps)
+constexpr int STAGES = 6;                  // bf16 operand stages in shared memory
+constexpr int PREF = 2;                    // stages of FP32 loads in flight per converter thread
+constexpr int NCONV = 512;                 // converter + epilogue threads (16 warps)
 constexpr int NTHREADS = NCONV + 32;       // + one MMA-issue warp
 constexpr int TILE_BYTES = BM * BK * 2;    // one bf16 operand tile (hi or lo): 8 KB
 constexpr int STAGE_BYTES = 4 * TILE_BYTES;  // A hi, A lo, B hi, B lo
@@ -138,17 +140,21 @@ __device__ __forceinline__ int64_t goff(int64_t i, int n, const int64_t* ext, co
   return mode_offset(i, n, ext, str);
 }
 
-// hi = bf16(x), lo = bf16(x - hi) for 8 values -> 16 B each.
+// hi = bf16_rn(x), lo = bf16_rn(x - hi) for 8 values -> 16 B each.  Packed:
+// one cvt.rn.bf16x2 per pair, hi widened back by bit shifts, x - hi by one
+// packed FMA (exact).  Non-finite inputs give a NaN residual (use the FP32
+// path for IEEE infinities).
 __device__ __forceinline__ void split8(const float (&v)[8], uint4& hi, uint4& lo) {
   uint32_t h[4], l[4];
 #pragma unroll
   for (int p = 0; p < 4; ++p) {
-    __nv_bfloat162 hb = __float22bfloat162_rn(make_float2(v[2 * p], v[2 * p + 1]));
-    float2 hf = __bfloat1622float2(hb);
-    float r0 = isfinite(hf.x) ? v[2 * p] - hf.x : 0.f;
-    float r1 = isfinite(hf.y) ? v[2 * p + 1] - hf.y : 0.f;
-    __nv_bfloat162 lb = __float22bfloat162_rn(make_float2(r0, r1));
-    h[p] = *reinterpret_cast<uint32_t*>(&hb);
+    const float2 x = make_float2(v[2 * p], v[2 * p + 1]);
+    __nv_bfloat162 hb = __float22bfloat162_rn(x);
+    const uint32_t hu = *reinterpret_cast<uint32_t*>(&hb);
+    const float2 hf = make_float2(__uint_as_float(hu << 16), __uint_as_float(hu & 0xffff0000u));
+    const float2 r = __ffma2_rn(hf, make_float2(-1.f, -1.f), x);
+    __nv_bfloat162 lb = __float22bfloat162_rn(r);
+    h[p] = hu;
     l[p] = *reinterpret_cast<uint32_t*>(&lb);
   }
   hi = make_uint4(h[0], h[1], h[2], h[3]);
@@ -166,18 +172,27 @@ __device__ __forceinline__ void load_unit(const float* __restrict__ base, int64_
     for (int i = 0; i < 8; ++i) v[i] = 0.f;
     return;
   }
-  if (kfast && k0 + 8 <= kend) {
-    const float* p = base + rowoff + goff(k0, nk, kext, kstr);
-    if ((reinterpret_cast<uintptr_t>(p) & 15) == 0) {
-      const float4 a = __ldg(reinterpret_cast<const float4*>(p));
-      const float4 b = __ldg(reinterpret_cast<const float4*>(p) + 1);
-      v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w;
-      v[4] = b.x; v[5] = b.y; v[6] = b.z; v[7] = b.w;
-    } else {
+  if (k0 + 8 <= kend) {
+    if (kfast) {
+      const float* p = base + rowoff + goff(k0, nk, kext, kstr);
+      if ((reinterpret_cast<uintptr_t>(p) & 15) == 0) {
+        const float4 a = __ldg(reinterpret_cast<const float4*>(p));
+        const float4 b = __ldg(reinterpret_cast<const float4*>(p) + 1);
+        v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w;
+        v[4] = b.x; v[5] = b.y; v[6] = b.z; v[7] = b.w;
+      } else {
 #pragma unroll
-      for (int i = 0; i < 8; ++i) v[i] = __ldg(p + i);
+        for (int i = 0; i < 8; ++i) v[i] = __ldg(p + i);
+      }
+      return;
     }
-    return;
+    if (nk == 1) {
+      const int64_t sk = kstr[0];
+      const float* p = base + rowoff + k0 * sk;
+#pragma unroll
+      for (int i = 0; i < 8; ++i) v[i] = __ldg(p + i * sk);
+      return;
+    }
   }
 #pragma unroll
   for (int i = 0; i < 8; ++i) {
@@ -186,7 +201,12 @@ __device__ __forceinline__ void load_unit(const float* __restrict__ base, int64_
   }
 }
 
-__global__ void __launch_bounds__(tc::NTHREADS, 2) k_gemm_bf16x3(const __grid_constant__ TcArgs t) {
+__device__ __forceinline__ void sts128(uint32_t addr, const uint4& v) {
+  asm volatile("st.shared.v4.b32 [%0], {%1, %2, %3, %4};" ::"r"(addr), "r"(v.x), "r"(v.y), "r"(v.z), "r"(v.w)
+               : "memory");
+}
+
+__global__ void __launch_bounds__(tc::NTHREADS, 1) k_gemm_bf16x3(const __grid_constant__ TcArgs t) {
   using namespace tc;
   extern __shared__ __align__(1024) unsigned char smem[];
   uint64_t* full = reinterpret_cast<uint64_t*>(smem + STAGES * STAGE_BYTES);
@@ -215,7 +235,7 @@ __global__ void __launch_bounds__(tc::NTHREADS, 2) k_gemm_bf16x3(const __grid_co
     *abort_flag = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
-  if (warp == NCONV / 32) {
+  if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
                  "r"(TMEM_COLS)
                  : "memory");
@@ -233,90 +253,75 @@ __global__ void __launch_bounds__(tc::NTHREADS, 2) k_gemm_bf16x3(const __grid_co
 
   if (warp < NCONV / 32) {
     // ---------------- converters ----------------
-    // unit u in {0,1} of each operand: (row, kchunk) of the 128 x 32 tile
-    int arow[2], akc[2], brow[2], bkc[2];
-    if (t.a_kfast) {
-      arow[0] = tid >> 2; arow[1] = (tid >> 2) + 64; akc[0] = akc[1] = tid & 3;
-    } else {
-      arow[0] = arow[1] = tid & 127; akc[0] = (tid >> 7) * 2; akc[1] = akc[0] + 1;
-    }
-    if (t.b_kfast) {
-      brow[0] = tid >> 2; brow[1] = (tid >> 2) + 64; bkc[0] = bkc[1] = tid & 3;
-    } else {
-      brow[0] = brow[1] = tid & 127; bkc[0] = (tid >> 7) * 2; bkc[1] = bkc[0] + 1;
-    }
-    int64_t aoff[2], boff[2];
-#pragma unroll
-    for (int u = 0; u < 2; ++u) {
-      const int64_t m = m0 + arow[u], n = n0 + brow[u];
-      aoff[u] = m < g.M ? la + goff(m, g.nm, g.m_ext, g.m_sa) : -1;
-      boff[u] = n < g.N ? lb + goff(n, g.nn, g.n_ext, g.n_sb) : -1;
-    }
-    // shared-memory byte offsets of each unit inside an operand tile
-    uint32_t aso[2], bso[2];
-#pragma unroll
-    for (int u = 0; u < 2; ++u) {
-      aso[u] = (uint32_t)((((arow[u] >> 3) * 4 + akc[u]) * 8 + (arow[u] & 7)) * 16);
-      bso[u] = (uint32_t)((((brow[u] >> 3) * 4 + bkc[u]) * 8 + (brow[u] & 7)) * 16);
-    }
-    float va[2][8], vb[2][8];
-    auto load_stage = [&](int kt) {
-      const int64_t kb = kbeg + (int64_t)kt * BK;
-#pragma unroll
-      for (int u = 0; u < 2; ++u) {
-        load_unit(Ap, aoff[u], kb + akc[u] * 8, kend, t.a_kfast, g.nk, g.k_ext, g.k_sa, va[u]);
-        load_unit(Bp, boff[u], kb + bkc[u] * 8, kend, t.b_kfast, g.nk, g.k_ext, g.k_sb, vb[u]);
+    // One unit (8 consecutive k of one row) of each operand per thread and
+    // stage.  K-contiguous operand: a warp covers 8 rows x 4 k-chunks (each
+    // row's 128 B read by 4 lanes); otherwise 32 consecutive rows of one
+    // k-chunk.  Either way each quarter-warp stores 8 rows of one k-chunk =
+    // one contiguous 128-byte core matrix (no bank conflicts).
+    int arow, akc, brow, bkc;
+    if (t.a_kfast) { arow = 8 * warp + (lane & 7); akc = lane >> 3; }
+    else { arow = 32 * (warp & 3) + lane; akc = warp >> 2; }
+    if (t.b_kfast) { brow = 8 * warp + (lane & 7); bkc = lane >> 3; }
+    else { brow = 32 * (warp & 3) + lane; bkc = warp >> 2; }
+    const int64_t am = m0 + arow, bn = n0 + brow;
+    const int64_t aoff = am < g.M ? la + goff(am, g.nm, g.m_ext, g.m_sa) : -1;
+    const int64_t boff = bn < g.N ? lb + goff(bn, g.nn, g.n_ext, g.n_sb) : -1;
+    const uint32_t aso = (uint32_t)((((arow >> 3) * 4 + akc) * 8 + (arow & 7)) * 16);
+    const uint32_t bso = (uint32_t)((((brow >> 3) * 4 + bkc) * 8 + (brow & 7)) * 16);
+    const uint32_t sbase = smem_u32(smem);
+
+    float ring[PREF + 1][2][8];
+    auto load_stage = [&](int kt, float (&dst)[2][8]) {
+      if (kt < nkt) {
+        const int64_t kb = kbeg + (int64_t)kt * BK;
+        load_unit(Ap, aoff, kb + akc * 8, kend, t.a_kfast, g.nk, g.k_ext, g.k_sa, dst[0]);
+        load_unit(Bp, boff, kb + bkc * 8, kend, t.b_kfast, g.nk, g.k_ext, g.k_sb, dst[1]);
       }
     };
-    if (nkt > 0) load_stage(0);
-    for (int kt = 0; kt < nkt; ++kt) {
-      float ca[2][8], cb[2][8];
-#pragma unroll
-      for (int u = 0; u < 2; ++u)
-#pragma unroll
-        for (int i = 0; i < 8; ++i) {
-          ca[u][i] = va[u][i];
-          cb[u][i] = vb[u][i];
-        }
-      if (kt + 1 < nkt) load_stage(kt + 1);  // prefetch the next stage into registers
+    auto convert_stage = [&](int kt, const float (&src)[2][8]) {
       const int s = kt % STAGES;
       if (kt >= STAGES) mbar_wait(&empty[s], (uint32_t)((kt / STAGES - 1) & 1), abort_flag);
-      unsigned char* st = smem + s * STAGE_BYTES;
-#pragma unroll
-      for (int u = 0; u < 2; ++u) {
-        uint4 hi, lo;
-        split8(ca[u], hi, lo);
-        *reinterpret_cast<uint4*>(st + aso[u]) = hi;
-        *reinterpret_cast<uint4*>(st + TILE_BYTES + aso[u]) = lo;
-        split8(cb[u], hi, lo);
-        *reinterpret_cast<uint4*>(st + 2 * TILE_BYTES + bso[u]) = hi;
-        *reinterpret_cast<uint4*>(st + 3 * TILE_BYTES + bso[u]) = lo;
-      }
+      const uint32_t st = sbase + s * STAGE_BYTES;
+      uint4 hi, lo;
+      split8(src[0], hi, lo);
+      sts128(st + aso, hi);
+      sts128(st + TILE_BYTES + aso, lo);
+      split8(src[1], hi, lo);
+      sts128(st + 2 * TILE_BYTES + bso, hi);
+      sts128(st + 3 * TILE_BYTES + bso, lo);
       fence_proxy_async();
       mbar_arrive(&full[s]);
+    };
+#pragma unroll
+    for (int p = 0; p < PREF; ++p) load_stage(p, ring[p]);
+    for (int kt = 0; kt < nkt; kt += PREF + 1) {
+#pragma unroll
+      for (int j = 0; j <= PREF; ++j) {
+        if (kt + j < nkt) {
+          load_stage(kt + j + PREF, ring[(j + PREF) % (PREF + 1)]);
+          convert_stage(kt + j, ring[j]);
+        }
+      }
     }
     // ---------------- epilogue ----------------
     const bool ok = nkt > 0 && mbar_wait(done, 0, abort_flag);
     tc_fence_after();
-    const int q = warp & 3, h = warp >> 2;
+    const int q = warp & 3, col = 32 * (warp >> 2);
     const int64_t m = m0 + 32 * q + lane;
     const bool mok = m < g.M;
     const int64_t lc = mode_offset(l, g.nl, g.l_ext, g.l_sc);
     const int64_t cm = mok ? goff(m, g.nm, g.m_ext, g.m_sc) : 0;
     float* Cp = static_cast<float*>(g.C);
     const float sx = scalar_as<float>(g.sx), sy = scalar_as<float>(g.sy);
-#pragma unroll 1
-    for (int c = 0; c < 2; ++c) {
-      uint32_t r[32];
-      const int col = 64 * h + 32 * c;
-      __syncwarp();
-      tmem_ld32(tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)col, r);
-      if (!ok) {
+    uint32_t r[32];
+    __syncwarp();
+    tmem_ld32(tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)col, r);
+    if (!ok) {
 #pragma unroll
-        for (int j = 0; j < 32; ++j) r[j] = 0u;
-      }
-      if (!mok) continue;
-#pragma unroll 4
+      for (int j = 0; j < 32; ++j) r[j] = 0u;
+    }
+    if (mok) {
+#pragma unroll
       for (int j = 0; j < 32; ++j) {
         const int64_t n = n0 + col + j;
         if (n >= g.N) break;
@@ -332,12 +337,13 @@ __global__ void __launch_bounds__(tc::NTHREADS, 2) k_gemm_bf16x3(const __grid_co
       }
     }
   } else if (lane == 0) {
-    // ---------------- MMA issue (one thread) ----------------
+    // ---------------- MMA issue (one thread of the last warp) ----------------
+    const uint32_t sbase = smem_u32(smem);
     for (int kt = 0; kt < nkt; ++kt) {
       const int s = kt % STAGES;
       if (!mbar_wait(&full[s], (uint32_t)((kt / STAGES) & 1), abort_flag)) break;
       tc_fence_after();
-      const uint32_t sb = smem_u32(smem + s * STAGE_BYTES);
+      const uint32_t sb = sbase + s * STAGE_BYTES;
 #pragma unroll
       for (int kk = 0; kk < 2; ++kk) {
         const uint32_t off = kk * 256;
@@ -353,7 +359,7 @@ __global__ void __launch_bounds__(tc::NTHREADS, 2) k_gemm_bf16x3(const __grid_co
   }
   tc_fence_before();
   __syncthreads();
-  if (warp == NCONV / 32) {
+  if (warp == 0) {
     tc_fence_after();
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TMEM_COLS) : "memory");
   }
@@ -402,12 +408,12 @@ cudaError_t launch_gemm_bf16x3(const GemmArgs& g, void* workspace, size_t ws_byt
   t.b_kfast = g.k_sb[0] == 1 && g.k_ext[0] % 8 == 0;
   const int64_t tm = (g.M + BM - 1) / BM, tn = (g.N + BN - 1) / BN;
   const int64_t tiles = tm * tn * g.L;
-  // split K until the grid covers the SMs twice (two CTAs per SM), keeping
-  // at least 8 k-steps per split
+  // split K until the grid covers the SMs (one CTA per SM), keeping at
+  // least 8 k-steps per split
   int64_t S = 1;
   const int64_t ksteps = (g.K + BK - 1) / BK;
-  if (tiles < 2 * num_sms) {
-    S = (2 * num_sms + tiles - 1) / tiles;
+  if (tiles < num_sms) {
+    S = (num_sms + tiles - 1) / tiles;
     S = std::min<int64_t>(S, std::max<int64_t>(1, ksteps / 8));
   }
   int64_t kchunk = ((ksteps + S - 1) / S) * BK;

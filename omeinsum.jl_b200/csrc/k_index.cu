@@ -211,6 +211,85 @@ __global__ void __launch_bounds__(256) k_loop_finish(const __grid_constant__ Loo
   }
 }
 
+// Reduction of one input whose first summed mode is contiguous (Sum over a
+// leading dimension, src/unaryrules.jl:30-40).  Inner space = E0 contiguous
+// elements x R rows (at most one more summed mode, row stride rs).  One block
+// per (output, row split); 16-byte vector loads when VEC (every row start
+// 16-byte aligned and E0 a multiple of the vector width), 4 loads in flight.
+template <class A, bool VEC>
+__global__ void __launch_bounds__(256) k_reduce_contig(const __grid_constant__ LoopArgs a, int64_t rchunk) {
+  using T = typename A::T;
+  constexpr int V = VEC ? (16 / sizeof(T) > 0 ? 16 / sizeof(T) : 1) : 1;
+  constexpr int U = 4;
+  __shared__ T sh[32];
+  const T sx = scalar_as<T>(a.sx), sy = scalar_as<T>(a.sy);
+  const T* x = static_cast<const T*>(a.x[0]);
+  const int64_t e0 = a.ext[a.nout];
+  const int64_t R = a.ninner > 1 ? a.ext[a.nout + 1] : 1;
+  const int64_t rs = a.ninner > 1 ? a.str[1][a.nout + 1] : 0;
+  const int64_t chunks = e0 / V;              // vector units per row
+  const int64_t nblocks = a.n_out * a.nsplit;
+  for (int64_t b = blockIdx.x; b < nblocks; b += gridDim.x) {
+    const int64_t o = b / a.nsplit;
+    const int64_t split = b - o * a.nsplit;
+    int64_t off[1];
+    const int64_t yoff = loop_outer_offsets<1>(a, o, off);
+    const int64_t rbeg = split * rchunk;
+    const int64_t rend = min(R, rbeg + rchunk);
+    const int64_t units = (rend - rbeg) * chunks;
+    T acc = A::zero();
+    for (int64_t u0 = threadIdx.x; u0 < units; u0 += (int64_t)blockDim.x * U) {
+      T part[U][V];
+#pragma unroll
+      for (int j = 0; j < U; ++j) {
+        const int64_t u = u0 + (int64_t)j * blockDim.x;
+        if (u < units) {
+          const int64_t r = rbeg + u / chunks;
+          const int64_t c = u - (u / chunks) * chunks;
+          const T* p = x + off[0] + r * rs + c * V;
+          if constexpr (VEC) {
+            const uint4 w = __ldg(reinterpret_cast<const uint4*>(p));
+            memcpy(&part[j][0], &w, sizeof(w));
+          } else {
+            part[j][0] = p[0];
+          }
+        } else {
+#pragma unroll
+          for (int v = 0; v < V; ++v) part[j][v] = A::zero();
+        }
+      }
+#pragma unroll
+      for (int j = 0; j < U; ++j)
+#pragma unroll
+        for (int v = 0; v < V; ++v) acc = A::add(acc, part[j][v]);
+    }
+    acc = block_reduce<A>(acc, sh);
+    if (threadIdx.x == 0) {
+      if (a.nsplit == 1) {
+        T* yp = static_cast<T*>(a.y) + yoff;
+        *yp = epilogue<A>(acc, yp, sx, sy, a.sy_zero, a.sx_one);
+      } else {
+        static_cast<T*>(a.partial)[b] = acc;
+      }
+    }
+  }
+}
+
+template <class A>
+static cudaError_t launch_reduce_contig_t(const LoopArgs& a, bool vec, int64_t rchunk, int grid, cudaStream_t s) {
+  if (vec) k_reduce_contig<A, true><<<grid, 256, 0, s>>>(a, rchunk);
+  else k_reduce_contig<A, false><<<grid, 256, 0, s>>>(a, rchunk);
+  count_launch();
+  return cudaGetLastError();
+}
+
+cudaError_t launch_reduce_contig(ome_dtype dt, const LoopArgs& a, bool vec, int64_t rchunk, int grid,
+                                 cudaStream_t s) {
+  cudaError_t e = cudaErrorInvalidValue;
+  OME_DISPATCH(dt, ALG, e = launch_reduce_contig_t<ALG>(a, vec, rchunk, grid, s));
+  return e;
+}
+
 template <class A>
 static cudaError_t launch_loop_t(const LoopArgs& a, LoopMode mode, int grid, int block,
                                  cudaStream_t s) {
@@ -251,22 +330,24 @@ cudaError_t launch_loop_finish(ome_dtype dt, const LoopArgs& a, cudaStream_t s) 
 // permute / broadcast copy
 // ---------------------------------------------------------------------------
 
-// 32x32 tile transpose between y's fastest mode (mode 0) and x's fastest
-// mode (tmode); every other mode is a batch index.  Reads are coalesced
-// along x's contiguous mode, writes along y's.  256 threads = 32 x 8.
-template <class A>
+// Tile transpose between y's fastest mode (mode 0) and x's fastest mode
+// (tmode); every other mode is a batch index.  Tile = 32 (x-fast) x TY
+// (y-fast).  Reads are coalesced along x's contiguous mode, writes along y's;
+// each thread keeps TY/8 elements in flight.  256 threads = 32 x 8.
+template <class A, int TY>
 __global__ void __launch_bounds__(256) k_transpose(const __grid_constant__ PermArgs a) {
   using T = typename A::T;
-  __shared__ T tile[32][33];
+  __shared__ T tile[TY][33];
   const T sx = scalar_as<T>(a.sx), sy = scalar_as<T>(a.sy);
   const int tmode = a.tmode;
   const int64_t e0 = a.ext[0], et = a.ext[tmode];
-  const int64_t t0 = (e0 + 31) >> 5, tt = (et + 31) >> 5;
+  const int64_t t0 = (e0 + TY - 1) / TY, tt = (et + 31) >> 5;
   const int64_t nbatch = a.n / (e0 * et);
   const int64_t ntiles = t0 * tt * nbatch;
   const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
   const T* x = static_cast<const T*>(a.x);
   T* y = static_cast<T*>(a.y);
+  const int64_t xs0 = a.xs[0], xst = a.xs[tmode], ys0 = a.ys[0], yst = a.ys[tmode];
   for (int64_t tid = blockIdx.x; tid < ntiles; tid += gridDim.x) {
     int64_t r = tid;
     const int64_t i0 = r % t0;
@@ -284,19 +365,30 @@ __global__ void __launch_bounds__(256) k_transpose(const __grid_constant__ PermA
       yb += d * a.ys[m];
     }
     const int64_t p = it * 32 + tx;
+    const bool pin = p < et;
+    const T* xp = x + xb + p * xst;
+    T v[TY / 8];
 #pragma unroll
-    for (int k = 0; k < 4; ++k) {
-      const int64_t q = i0 * 32 + ty + 8 * k;
-      if (p < et && q < e0) tile[ty + 8 * k][tx] = x[xb + p * a.xs[tmode] + q * a.xs[0]];
+    for (int k = 0; k < TY / 8; ++k) {
+      const int64_t q = i0 * TY + ty + 8 * k;
+      v[k] = (pin && q < e0) ? xp[q * xs0] : A::zero();
     }
-    __syncthreads();
-    const int64_t q = i0 * 32 + tx;
 #pragma unroll
-    for (int k = 0; k < 4; ++k) {
-      const int64_t pp = it * 32 + ty + 8 * k;
-      if (pp < et && q < e0) {
-        T* yp = y + yb + q * a.ys[0] + pp * a.ys[tmode];
-        *yp = epilogue<A>(tile[tx][ty + 8 * k], yp, sx, sy, a.sy_zero, a.sx_one);
+    for (int k = 0; k < TY / 8; ++k) tile[ty + 8 * k][tx] = v[k];
+    __syncthreads();
+#pragma unroll
+    for (int h = 0; h < TY / 32; ++h) {
+      const int64_t q = i0 * TY + 32 * h + tx;
+      if (q < e0) {
+        T* yq = y + yb + q * ys0;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+          const int64_t pp = it * 32 + ty + 8 * k;
+          if (pp < et) {
+            T* yp = yq + pp * yst;
+            *yp = epilogue<A>(tile[32 * h + tx][ty + 8 * k], yp, sx, sy, a.sy_zero, a.sx_one);
+          }
+        }
       }
     }
     __syncthreads();
@@ -363,10 +455,11 @@ static cudaError_t launch_perm_t(const PermArgs& a, int num_sms, cudaStream_t s)
   if (a.n == 0) return cudaSuccess;
   const int maxgrid = num_sms * 16;
   if (a.tmode > 0) {
-    const int64_t tiles = ((a.ext[0] + 31) / 32) * ((a.ext[a.tmode] + 31) / 32) *
+    constexpr int TY = sizeof(T) <= 4 ? 64 : 32;
+    const int64_t tiles = ((a.ext[0] + TY - 1) / TY) * ((a.ext[a.tmode] + 31) / 32) *
                           (a.n / (a.ext[0] * a.ext[a.tmode]));
     const int grid = (int)(tiles < maxgrid ? tiles : maxgrid);
-    k_transpose<A><<<grid, 256, 0, s>>>(a); count_launch();
+    k_transpose<A, TY><<<grid, 256, 0, s>>>(a); count_launch();
   } else if (a.nd == 1 && a.xs[0] == 1 && a.ys[0] == 1 && sizeof(T) <= 16 && 16 % sizeof(T) == 0 &&
              ((uintptr_t)a.x % 16) == 0 && ((uintptr_t)a.y % 16) == 0) {
     const int64_t nb = (a.n / (16 / sizeof(T)) + 255) / 256;

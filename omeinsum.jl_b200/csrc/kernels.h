@@ -17,6 +17,10 @@ enum LoopMode { LOOP_THREAD = 0, LOOP_BLOCK = 1 };
 cudaError_t launch_loop(ome_dtype dt, const LoopArgs& a, LoopMode mode, int grid, int block,
                         cudaStream_t s);
 cudaError_t launch_loop_finish(ome_dtype dt, const LoopArgs& a, cudaStream_t s);
+// One input, first inner mode contiguous, at most one more inner mode: block
+// per (output, row split) with vector loads (vec) over rows of rchunk.
+cudaError_t launch_reduce_contig(ome_dtype dt, const LoopArgs& a, bool vec, int64_t rchunk, int grid,
+                                 cudaStream_t s);
 
 // Permute / broadcast / identity copy with the αβ epilogue.
 cudaError_t launch_perm(ome_dtype dt, const PermArgs& a, int num_sms, cudaStream_t s);
