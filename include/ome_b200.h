@@ -169,6 +169,31 @@ OME_API int ome_plan_gradient(ome_ctx* ctx, ome_plan* plan, void* stream,
                       const void* const* inputs, const void* dy, void* y,
                       void* const* dxs);
 
+/* Allocation-free reduction --------------------------------------------------
+ *
+ * No counterpart in the reference.  y <- sy*y + sx*sum(x) where every label
+ * of y is a label of x and the labels of x missing from y are summed (a Sum
+ * or Tr einsum such as "ii->" or "ijk->j"; repeated input labels are
+ * diagonals).  It runs the same two-pass split reduction as ome_einsum, but
+ * keeps the partial sums in a fixed array inside the library instead of a
+ * context workspace: it takes no context and allocates no device memory.
+ * For callers that cannot let a library cudaMalloc: code whose device memory
+ * is owned by its own allocator (CUDA.jl's pool, a serving process with a
+ * fixed HBM arena), where an extra allocation would fail or fragment the
+ * budget and cudaMalloc/cudaFree would synchronise the device.
+ *
+ * Limit: the partial sums (at least two per output element) must fit in
+ * OME_NOALLOC_SCRATCH_BYTES, i.e. at most OME_NOALLOC_SCRATCH_BYTES /
+ * (2 * element size) output elements; larger outputs are rejected with
+ * OME_UNSUPPORTED.  Every GPU that loads the library holds the array until
+ * the process exits.  The first call on a device looks up the array's device
+ * address with that device current; make it before any stream capture.
+ * All calls on a device share the array: calls that overlap on the GPU
+ * (different streams or host threads) race and must be serialised. */
+#define OME_NOALLOC_SCRATCH_BYTES (4u << 20)
+OME_API int ome_reduce_noalloc(void* stream, ome_dtype dtype, const ome_tensor* x,
+                               const ome_tensor* y, const void* sx, const void* sy);
+
 #ifdef __cplusplus
 }
 #endif

@@ -22,7 +22,7 @@ PREC_AUTO, PREC_FP32, PREC_BF16X3 = range(3)
 EXPORTS = [
     "ome_version", "ome_launch_count", "ome_device_status", "ome_last_error", "ome_ctx_create", "ome_ctx_destroy", "ome_ctx_workspace_bytes",
     "ome_einsum", "ome_loop_einsum", "ome_plan_create", "ome_plan_destroy", "ome_plan_peak_bytes",
-    "ome_plan_execute", "ome_plan_gradient",
+    "ome_plan_execute", "ome_plan_gradient", "ome_reduce_noalloc",
 ]
 
 
@@ -83,6 +83,7 @@ def load() -> C.CDLL:
         lib.ome_plan_peak_bytes.argtypes = [P, C.POINTER(C.c_size_t), C.POINTER(C.c_size_t)]
         lib.ome_plan_execute.argtypes = [P, P, P, C.POINTER(P), P, P, P]
         lib.ome_plan_gradient.argtypes = [P, P, P, C.POINTER(P), P, P, C.POINTER(P)]
+        lib.ome_reduce_noalloc.argtypes = [P, C.c_int, C.POINTER(Tensor), C.POINTER(Tensor), P, P]
         for f in EXPORTS:
             if f not in ("ome_version", "ome_last_error", "ome_launch_count"):
                 getattr(lib, f).restype = C.c_int
