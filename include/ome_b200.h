@@ -63,13 +63,16 @@ typedef enum {
   OME_TROP_F64 = 7
 } ome_dtype;
 
-/* Precision mode for F32/C32 contractions.
- * OME_PREC_AUTO   : BF16x3 split products on the tensor cores where the
- *                   contraction is GEMM-shaped, exact-type CUDA-core code elsewhere.
+/* Precision mode for F32 contractions (other dtypes ignore it).
+ * GEMM-shaped F32 contractions run on the tensor cores as split BF16
+ * products accumulated in FP32: each value x = t0 + t1 (+ t2) in bf16.
+ * OME_PREC_AUTO   : BF16x6 (3 terms, 6 MMAs per K step; products exact to
+ *                   about 2^-24, i.e. FP32-faithful).
  * OME_PREC_FP32   : CUDA-core FP32 FMA everywhere (the plain GPU path).
- * OME_PREC_BF16X3 : same as AUTO.
- * Other dtypes ignore it. */
-typedef enum { OME_PREC_AUTO = 0, OME_PREC_FP32 = 1, OME_PREC_BF16X3 = 2 } ome_prec;
+ * OME_PREC_BF16X3 : 2 terms, 3 MMAs (hi*hi + hi*lo + lo*hi); products exact
+ *                   to about 2^-16 -- twice as fast, not FP32-accurate.
+ * OME_PREC_BF16X6 : same as AUTO. */
+typedef enum { OME_PREC_AUTO = 0, OME_PREC_FP32 = 1, OME_PREC_BF16X3 = 2, OME_PREC_BF16X6 = 3 } ome_prec;
 
 typedef struct {
   void* data;

@@ -17,7 +17,7 @@ OK, INVALID_ARGUMENT, DIMENSION_MISMATCH, UNSUPPORTED, OUT_OF_MEMORY, TIMEOUT, C
 # dtypes (ome_dtype)
 F32, F64, C32, C64, I64, BOOL, TROP_F32, TROP_F64 = range(8)
 # precision modes (ome_prec)
-PREC_AUTO, PREC_FP32, PREC_BF16X3 = range(3)
+PREC_AUTO, PREC_FP32, PREC_BF16X3, PREC_BF16X6 = range(4)
 
 EXPORTS = [
     "ome_version", "ome_launch_count", "ome_device_status", "ome_last_error", "ome_ctx_create", "ome_ctx_destroy", "ome_ctx_workspace_bytes",

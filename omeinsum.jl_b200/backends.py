@@ -32,9 +32,10 @@ class CuTensorBackend(EinsumBackend):
 class B200Backend(EinsumBackend):
     """The sm_100a backend of this package.
 
-    prec: 0 = AUTO (BF16x3 tensor-core split products for GEMM-shaped FP32
-    contractions), 1 = FP32 (CUDA-core FP32 everywhere, the plain GPU path),
-    2 = BF16X3 (same as AUTO).  Other element types ignore it.
+    prec (FP32 only): 0 = AUTO = 3 = BF16X6 (tensor-core products of a 3-term
+    bf16 split, FP32-faithful), 1 = FP32 (CUDA-core FP32 everywhere, the
+    plain GPU path), 2 = BF16X3 (2-term split: twice as fast, about 16-bit
+    products).  Other element types ignore it.
     """
 
     def __init__(self, prec: int = 0):

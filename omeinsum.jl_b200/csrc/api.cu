@@ -15,6 +15,7 @@
 //    labels (summed on one side only) are pre-reduced as the reference does.
 #include <stdarg.h>
 #include <stdio.h>
+#include <stdlib.h>
 #include <string.h>
 #include <algorithm>
 #include <string>
@@ -52,6 +53,28 @@ int cuda_err(cudaError_t e, const char* what) {
     cudaError_t e_ = (call);                           \
     if (e_ != cudaSuccess) return cuda_err(e_, what);  \
   } while (0)
+
+// ----------------------------------------------------------------------------
+// dispatch trace: OME_TRACE=1 in the environment logs every dispatch decision
+// with its device time (events + synchronize, so only for diagnosis)
+// ----------------------------------------------------------------------------
+
+static int trace_on() {
+  static int v = -1;
+  if (v < 0) {
+    const char* e = getenv("OME_TRACE");
+    v = (e && e[0] && e[0] != '0') ? 1 : 0;
+  }
+  return v;
+}
+static thread_local char g_trace[256];
+static void trace_path(const char* fmt, ...) {
+  if (!trace_on()) return;
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(g_trace, sizeof(g_trace), fmt, ap);
+  va_end(ap);
+}
 
 void* ws_alloc(ome_ctx* c, size_t bytes) {
   size_t off = (c->ws_top + 255) & ~(size_t)255;
@@ -298,12 +321,16 @@ static int run_loop(ome_ctx* ctx, cudaStream_t s, ome_dtype dt, int nin, const H
     }
     a.nsplit = (int)nsplit;
     const int grid = (int)std::min<int64_t>(n_out * nsplit, (int64_t)sms * 32);
+    trace_path("reduce_contig n_out=%lld n_in=%lld modes=%d+%d nsplit=%lld vec=%d", (long long)n_out,
+               (long long)n_in, outer.n, inner.n, (long long)nsplit, (int)vec);
     OME_CK(cuda_err(launch_reduce_contig(dt, a, vec, rchunk, grid, s), "reduce kernel"));
     if (nsplit > 1) OME_CK(cuda_err(launch_loop_finish(dt, a, s), "reduce finish"));
     return OME_OK;
   }
   const bool thread_mode = n_in <= 16 || n_out >= (int64_t)sms * 512;
   if (thread_mode) {
+    trace_path("loop_thread nin=%d n_out=%lld n_in=%lld modes=%d+%d", nin, (long long)n_out, (long long)n_in,
+               outer.n, inner.n);
     const int64_t nb = (n_out + 255) / 256;
     const int grid = (int)std::min<int64_t>(nb, (int64_t)sms * 16);
     return cuda_err(launch_loop(dt, a, LOOP_THREAD, grid, 256, s), "index kernel");
@@ -332,6 +359,8 @@ static int run_loop(ome_ctx* ctx, cudaStream_t s, ome_dtype dt, int nin, const H
   }
   const int64_t nblocks = n_out * nsplit;
   const int grid = (int)std::min<int64_t>(nblocks, (int64_t)sms * 32);
+  trace_path("loop_block nin=%d n_out=%lld n_in=%lld modes=%d+%d nsplit=%lld", nin, (long long)n_out,
+             (long long)n_in, outer.n, inner.n, (long long)nsplit);
   OME_CK(cuda_err(launch_loop(dt, a, LOOP_BLOCK, grid, block, s), "index kernel"));
   if (nsplit > 1) OME_CK(cuda_err(launch_loop_finish(dt, a, s), "index kernel finish"));
   return OME_OK;
@@ -389,6 +418,7 @@ static int run_unary(ome_ctx* ctx, cudaStream_t s, ome_dtype dt, const HView& xu
   for (int m = 0; m < a.nd; ++m)
     if (a.xs[m] == 1 || a.xs[m] == -1) { p = m; break; }
   if (p > 0 && (a.xs[0] > 1 || a.xs[0] < -1) && a.ext[0] >= 4 && a.ext[p] >= 4) a.tmode = p;
+  trace_path("permute n=%lld modes=%d tmode=%d", (long long)n, a.nd, a.tmode);
   return cuda_err(launch_perm(dt, a, ctx->num_sms, s), "permute kernel");
 }
 
@@ -491,16 +521,27 @@ static int run_binary(ome_ctx* ctx, cudaStream_t s, ome_dtype dt, HView x1, HVie
     g.sy = sy;
     g.sy_zero = sy_zero;
     g.sx_one = scalar_is_one(dt, sx);
-    if (dt == OME_F32 && prec != OME_PREC_FP32 && gemm_bf16x3_supported(g)) {
+    trace_path("gemm M=%lld N=%lld K=%lld L=%lld modes=%d/%d/%d/%d afast=%d bfast=%d prec=%d", (long long)M,
+               (long long)N, (long long)K, (long long)L, gm.n, gn.n, gk.n, gl.n, g.a_m_fast, g.b_n_fast, prec);
+    if (dt == OME_F32 && prec != OME_PREC_FP32 && gemm_split_supported(g)) {
       size_t avail = ctx->ws_bytes > ctx->ws_top ? ctx->ws_bytes - ((ctx->ws_top + 255) & ~(size_t)255) : 0;
       void* w = avail ? ctx->ws + ((ctx->ws_top + 255) & ~(size_t)255) : nullptr;
-      cudaError_t e = launch_gemm_bf16x3(g, w, avail, ctx->num_sms, s);
-      if (e != cudaErrorNotSupported) return cuda_err(e, "bf16x3 gemm");
+      const int nterms = prec == OME_PREC_BF16X3 ? 2 : 3;
+      cudaError_t e = launch_gemm_split(g, nterms, w, avail, ctx->num_sms, s);
+      if (e != cudaErrorNotSupported) return cuda_err(e, "bf16 split gemm");
       cudaGetLastError();
     }
     return cuda_err(launch_gemm_simt(dt, g, s), "simt gemm");
   }
   HView xs[2] = {x1, x2};
+  if (trace_on()) {
+    char buf[96];
+    snprintf(buf, sizeof(buf), " [binary M=%lld N=%lld K=%lld L=%lld]", (long long)M, (long long)N, (long long)K,
+             (long long)L);
+    int rc = run_loop(ctx, s, dt, 2, xs, yu, sx, sy, sy_zero);
+    strncat(g_trace, buf, sizeof(g_trace) - strlen(g_trace) - 1);
+    return rc;
+  }
   return run_loop(ctx, s, dt, 2, xs, yu, sx, sy, sy_zero);
 }
 
@@ -508,8 +549,8 @@ static int run_binary(ome_ctx* ctx, cudaStream_t s, ome_dtype dt, HView x1, HVie
 // einsum on labelled views
 // ----------------------------------------------------------------------------
 
-int einsum_views(ome_ctx* ctx, cudaStream_t s, ome_dtype dt, int nin, const HView* xs, const HView& y,
-                 const Scalar& sx, const Scalar& sy_in, int prec, bool loop_only) {
+static int einsum_views_impl(ome_ctx* ctx, cudaStream_t s, ome_dtype dt, int nin, const HView* xs,
+                             const HView& y, const Scalar& sx, const Scalar& sy_in, int prec, bool loop_only) {
   if (nin < 1) return set_err(OME_INVALID_ARGUMENT, "number of input tensors must be greater than 0");
   if (nin > MAXIN) return set_err(OME_UNSUPPORTED, "at most %d input tensors per contraction", MAXIN);
   // size dict consistency (get_size_dict!, src/interfaces.jl:75-94)
@@ -549,6 +590,27 @@ int einsum_views(ome_ctx* ctx, cudaStream_t s, ome_dtype dt, int nin, const HVie
   if (loop_only || nin >= 3) return run_loop(ctx, s, dt, nin, xu, yu, sx, sy, sy_zero);
   if (nin == 1) return run_unary(ctx, s, dt, xu[0], yu, sx, sy, sy_zero);
   return run_binary(ctx, s, dt, xu[0], xu[1], yu, sx, sy, sy_zero, prec);
+}
+
+int einsum_views(ome_ctx* ctx, cudaStream_t s, ome_dtype dt, int nin, const HView* xs, const HView& y,
+                 const Scalar& sx, const Scalar& sy, int prec, bool loop_only) {
+  if (!trace_on()) return einsum_views_impl(ctx, s, dt, nin, xs, y, sx, sy, prec, loop_only);
+  g_trace[0] = 0;
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  cudaEventRecord(e0, s);
+  const int rc = einsum_views_impl(ctx, s, dt, nin, xs, y, sx, sy, prec, loop_only);
+  cudaEventRecord(e1, s);
+  cudaEventSynchronize(e1);
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  fprintf(stderr, "[ome] dt=%d nin=%d ranks=", (int)dt, nin);
+  for (int i = 0; i < nin; ++i) fprintf(stderr, "%d,", xs[i].nd);
+  fprintf(stderr, "%d us=%.1f %s\n", y.nd, ms * 1e3, g_trace);
+  return rc;
 }
 
 }  // namespace ome

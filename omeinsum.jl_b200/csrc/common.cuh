@@ -11,9 +11,9 @@
 namespace ome {
 
 constexpr int MAXD = 64;     // max rank of a tensor at the ABI
-constexpr int MAXM = 32;     // max merged modes in one kernel launch
+constexpr int MAXM = 64;     // max merged modes in one kernel launch
 constexpr int MAXIN = 8;     // max inputs of one index-kernel launch
-constexpr int MAXG = 8;      // max merged modes per GEMM group (M, N, K, batch)
+constexpr int MAXG = 32;     // max merged modes per GEMM group (M, N, K, batch)
 
 // ---------------------------------------------------------------------------
 // element types

@@ -1,4 +1,5 @@
-// Tensor-core FP32 contraction from BF16x3 split products (sm_100a tcgen05).
+// Tensor-core FP32 contraction from BF16 split products (sm_100a tcgen05):
+// BF16x3 (2 terms per value, 3 MMAs) or BF16x6 (3 terms, 6 MMAs).
 //
 // Replaces the GEMM at the heart of OMEinsum's binary path
 // (src/einsum.jl:104-124 -> src/binaryrules.jl mul!/_batched_gemm!, on GPU
@@ -10,14 +11,19 @@
 //    absorbed in the addressing; nothing is written back to HBM);
 //  * 16 converter warps load FP32 from global memory (coalesced along the
 //    operand's contiguous mode), split each value x into hi = bf16(x) and
-//    lo = bf16(x - hi) and store both into shared memory in the UMMA K-major
+//    lo = bf16(x - hi) (and a third term for BF16x6) and store them into shared memory in the UMMA K-major
 //    no-swizzle canonical layout (8-row x 16-byte core matrices);
 //    with two stages of loads in flight per thread;
 //  * one elected thread of a seventeenth warp issues, per K=16 step, three
-//    tcgen05.mma kind::f16 (hi*hi + hi*lo + lo*hi) accumulating in FP32 in
+//    (BF16x3: hi*hi + hi*lo + lo*hi) or six (BF16x6: every term pair whose
+//    orders sum below 3) tcgen05.mma kind::f16 accumulating in FP32 in
 //    tensor memory; tcgen05.commit releases each shared-memory stage;
-//  * the converter warps then read the 128x128 FP32 accumulator from TMEM
-//    (tcgen05.ld) and apply the y <- sy*y + sx*f epilogue through the
+//  * TMEM holds two buffers of (main = t0*t0, cross = other term pairs)
+//    accumulators; every CHUNK k-steps the converter warps drain the finished
+//    buffer (tcgen05.ld) into FP32 running sums in shared memory with
+//    round-to-nearest CUDA-core adds -- the tensor core's accumulation then
+//    only ever spans CHUNK k-steps, which keeps BF16x6 FP32-faithful;
+//  * the epilogue applies the y <- sy*y + sx*f epilogue through the
 //    output's mode strides, or write a split-K partial that a second kernel
 //    sums in a fixed order (deterministic);
 //  * every mbarrier wait is bounded (about 2 s of %globaltimer); on expiry the
@@ -32,14 +38,18 @@ __device__ int g_ome_timeout = 0;
 
 namespace tc {
 constexpr int BM = 128, BN = 128, BK = 32;
-constexpr int STAGES = 6;                  // bf16 operand stages in shared memory
+constexpr int CHUNK = 8;                   // k-steps accumulated in TMEM between drains
+constexpr int ACC_BYTES = BM * BN * 4;     // FP32 running sums in shared memory
+template <int NT> struct Cfg {             // NT = bf16 terms per value (2: BF16x3, 3: BF16x6)
+  static constexpr int STAGE_BYTES = 2 * NT * BM * BK * 2;   // A terms then B terms
+  static constexpr int STAGES = NT == 2 ? 4 : 3;
+  static constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + ACC_BYTES + 256;
+};
 constexpr int PREF = 2;                    // stages of FP32 loads in flight per converter thread
 constexpr int NCONV = 512;                 // converter + epilogue threads (16 warps)
 constexpr int NTHREADS = NCONV + 32;       // + one MMA-issue warp
-constexpr int TILE_BYTES = BM * BK * 2;    // one bf16 operand tile (hi or lo): 8 KB
-constexpr int STAGE_BYTES = 4 * TILE_BYTES;  // A hi, A lo, B hi, B lo
-constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 256;
-constexpr int TMEM_COLS = 128;
+constexpr int TILE_BYTES = BM * BK * 2;    // one bf16 operand tile (one term): 8 KB
+constexpr int TMEM_COLS = 512;            // 2 buffers x (main, cross-term) 128-column accumulators
 constexpr unsigned long long WAIT_NS = 2000000000ull;
 // kind::f16, BF16 x BF16 -> F32, K-major A and B, M = 128, N = 128
 constexpr uint32_t IDESC = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(BN >> 3) << 17) |
@@ -122,6 +132,15 @@ __device__ __forceinline__ void umma_commit(uint64_t* bar) {
                    smem_u32(bar))
                : "memory");
 }
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&r)[16]) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
+      "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
 __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&r)[32]) {
   asm volatile(
       "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
@@ -140,25 +159,30 @@ __device__ __forceinline__ int64_t goff(int64_t i, int n, const int64_t* ext, co
   return mode_offset(i, n, ext, str);
 }
 
-// hi = bf16_rn(x), lo = bf16_rn(x - hi) for 8 values -> 16 B each.  Packed:
-// one cvt.rn.bf16x2 per pair, hi widened back by bit shifts, x - hi by one
-// packed FMA (exact).  Non-finite inputs give a NaN residual (use the FP32
-// path for IEEE infinities).
-__device__ __forceinline__ void split8(const float (&v)[8], uint4& hi, uint4& lo) {
-  uint32_t h[4], l[4];
+// Split 8 values into NT bf16 terms, x ~ t0 + t1 (+ t2): t0 = bf16_rn(x),
+// t1 = bf16_rn(x - t0), t2 = bf16_rn(x - t0 - t1); 16 B per term.  Packed:
+// one cvt.rn.bf16x2 per pair and term, terms widened back by bit shifts,
+// residuals by one packed FMA each (exact).  Non-finite inputs give NaN
+// residuals (the FP32 path keeps IEEE infinities).
+template <int NT>
+__device__ __forceinline__ void split8(const float (&v)[8], uint4 (&out)[NT]) {
+  uint32_t w[NT][4];
 #pragma unroll
   for (int p = 0; p < 4; ++p) {
-    const float2 x = make_float2(v[2 * p], v[2 * p + 1]);
-    __nv_bfloat162 hb = __float22bfloat162_rn(x);
-    const uint32_t hu = *reinterpret_cast<uint32_t*>(&hb);
-    const float2 hf = make_float2(__uint_as_float(hu << 16), __uint_as_float(hu & 0xffff0000u));
-    const float2 r = __ffma2_rn(hf, make_float2(-1.f, -1.f), x);
-    __nv_bfloat162 lb = __float22bfloat162_rn(r);
-    h[p] = hu;
-    l[p] = *reinterpret_cast<uint32_t*>(&lb);
+    float2 r = make_float2(v[2 * p], v[2 * p + 1]);
+#pragma unroll
+    for (int t = 0; t < NT; ++t) {
+      __nv_bfloat162 b = __float22bfloat162_rn(r);
+      const uint32_t u = *reinterpret_cast<uint32_t*>(&b);
+      w[t][p] = u;
+      if (t + 1 < NT) {
+        const float2 bf = make_float2(__uint_as_float(u << 16), __uint_as_float(u & 0xffff0000u));
+        r = __ffma2_rn(bf, make_float2(-1.f, -1.f), r);
+      }
+    }
   }
-  hi = make_uint4(h[0], h[1], h[2], h[3]);
-  lo = make_uint4(l[0], l[1], l[2], l[3]);
+#pragma unroll
+  for (int t = 0; t < NT; ++t) out[t] = make_uint4(w[t][0], w[t][1], w[t][2], w[t][3]);
 }
 
 // Load one unit: 8 consecutive k (k0 .. k0+7) of one row.  rowoff < 0: a row
@@ -206,13 +230,17 @@ __device__ __forceinline__ void sts128(uint32_t addr, const uint4& v) {
                : "memory");
 }
 
+template <int NT>
 __global__ void __launch_bounds__(tc::NTHREADS, 1) k_gemm_bf16x3(const __grid_constant__ TcArgs t) {
   using namespace tc;
+  constexpr int STAGES = Cfg<NT>::STAGES, STAGE_BYTES = Cfg<NT>::STAGE_BYTES;
   extern __shared__ __align__(1024) unsigned char smem[];
-  uint64_t* full = reinterpret_cast<uint64_t*>(smem + STAGES * STAGE_BYTES);
+  float* acc = reinterpret_cast<float*>(smem + STAGES * STAGE_BYTES);   // [BN][BM] running sums
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem + STAGES * STAGE_BYTES + ACC_BYTES);
   uint64_t* empty = full + STAGES;
-  uint64_t* done = empty + STAGES;
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(done + 1);
+  uint64_t* chunk_done = empty + STAGES;   // [2]: a TMEM buffer's chunk of MMAs completed
+  uint64_t* drained = chunk_done + 2;      // [2]: the converters have read that buffer
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(drained + 2);
   volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
 
   const GemmArgs& g = t.g;
@@ -225,17 +253,21 @@ __global__ void __launch_bounds__(tc::NTHREADS, 1) k_gemm_bf16x3(const __grid_co
   const int64_t kbeg = split * t.kchunk;
   const int64_t kend = min(g.K, kbeg + t.kchunk);
   const int nkt = (int)((kend - kbeg + BK - 1) / BK);
+  const int nchunks = (nkt + CHUNK - 1) / CHUNK;
 
   if (tid == 0) {
     for (int s = 0; s < STAGES; ++s) {
       mbar_init(&full[s], NCONV);
       mbar_init(&empty[s], 1);
     }
-    mbar_init(done, 1);
+    for (int b = 0; b < 2; ++b) {
+      mbar_init(&chunk_done[b], 1);
+      mbar_init(&drained[b], NCONV);
+    }
     *abort_flag = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
-  if (warp == 0) {
+  if (warp == NCONV / 32) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
                  "r"(TMEM_COLS)
                  : "memory");
@@ -245,6 +277,9 @@ __global__ void __launch_bounds__(tc::NTHREADS, 1) k_gemm_bf16x3(const __grid_co
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem = *tmem_slot;
+  // TMEM buffer b: main accumulator (t0*t0) at column 256b, cross terms at 256b + 128
+  auto tmem_main = [&](int b) { return tmem + (uint32_t)(256 * b); };
+  auto tmem_cross = [&](int b) { return tmem + (uint32_t)(256 * b + 128); };
 
   const float* Ap = static_cast<const float*>(g.A);
   const float* Bp = static_cast<const float*>(g.B);
@@ -269,6 +304,33 @@ __global__ void __launch_bounds__(tc::NTHREADS, 1) k_gemm_bf16x3(const __grid_co
     const uint32_t aso = (uint32_t)((((arow >> 3) * 4 + akc) * 8 + (arow & 7)) * 16);
     const uint32_t bso = (uint32_t)((((brow >> 3) * 4 + bkc) * 8 + (brow & 7)) * 16);
     const uint32_t sbase = smem_u32(smem);
+    // accumulator lanes / columns of this thread (TMEM lane quarter = warp & 3)
+    const int q = warp & 3, col = 32 * (warp >> 2);
+    const int row = 32 * q + lane;
+
+    // Drain chunk c: its TMEM buffer -> the FP32 running sums in shared memory
+    // (round-to-nearest CUDA-core additions), then release the buffer.
+    int drained_chunks = 0;
+    auto drain = [&](int c) {
+      const int b = c & 1;
+      mbar_wait(&chunk_done[b], (uint32_t)((c >> 1) & 1), abort_flag);
+      tc_fence_after();
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        uint32_t rm[16], rc[16];
+        __syncwarp();
+        tmem_ld16(tmem_main(b) + ((uint32_t)(32 * q) << 16) + (uint32_t)(col + 16 * h), rm);
+        tmem_ld16(tmem_cross(b) + ((uint32_t)(32 * q) << 16) + (uint32_t)(col + 16 * h), rc);
+#pragma unroll
+        for (int j = 0; j < 16; ++j) {
+          const float v = __uint_as_float(rm[j]) + __uint_as_float(rc[j]);
+          float* a = acc + (col + 16 * h + j) * BM + row;
+          *a = c == 0 ? v : *a + v;
+        }
+      }
+      tc_fence_before();
+      mbar_arrive(&drained[b]);
+    };
 
     float ring[PREF + 1][2][8];
     auto load_stage = [&](int kt, float (&dst)[2][8]) {
@@ -279,16 +341,18 @@ __global__ void __launch_bounds__(tc::NTHREADS, 1) k_gemm_bf16x3(const __grid_co
       }
     };
     auto convert_stage = [&](int kt, const float (&src)[2][8]) {
+      // chunk c - 2 must be drained before the MMAs of chunk c reuse its buffer
+      if (kt % CHUNK == 0 && kt >= 2 * CHUNK) drain(drained_chunks++);
       const int s = kt % STAGES;
       if (kt >= STAGES) mbar_wait(&empty[s], (uint32_t)((kt / STAGES - 1) & 1), abort_flag);
       const uint32_t st = sbase + s * STAGE_BYTES;
-      uint4 hi, lo;
-      split8(src[0], hi, lo);
-      sts128(st + aso, hi);
-      sts128(st + TILE_BYTES + aso, lo);
-      split8(src[1], hi, lo);
-      sts128(st + 2 * TILE_BYTES + bso, hi);
-      sts128(st + 3 * TILE_BYTES + bso, lo);
+      uint4 terms[NT];
+      split8<NT>(src[0], terms);
+#pragma unroll
+      for (int u = 0; u < NT; ++u) sts128(st + u * TILE_BYTES + aso, terms[u]);
+      split8<NT>(src[1], terms);
+#pragma unroll
+      for (int u = 0; u < NT; ++u) sts128(st + (NT + u) * TILE_BYTES + bso, terms[u]);
       fence_proxy_async();
       mbar_arrive(&full[s]);
     };
@@ -303,29 +367,19 @@ __global__ void __launch_bounds__(tc::NTHREADS, 1) k_gemm_bf16x3(const __grid_co
         }
       }
     }
+    while (drained_chunks < nchunks) drain(drained_chunks++);
     // ---------------- epilogue ----------------
-    const bool ok = nkt > 0 && mbar_wait(done, 0, abort_flag);
-    tc_fence_after();
-    const int q = warp & 3, col = 32 * (warp >> 2);
-    const int64_t m = m0 + 32 * q + lane;
-    const bool mok = m < g.M;
-    const int64_t lc = mode_offset(l, g.nl, g.l_ext, g.l_sc);
-    const int64_t cm = mok ? goff(m, g.nm, g.m_ext, g.m_sc) : 0;
-    float* Cp = static_cast<float*>(g.C);
-    const float sx = scalar_as<float>(g.sx), sy = scalar_as<float>(g.sy);
-    uint32_t r[32];
-    __syncwarp();
-    tmem_ld32(tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)col, r);
-    if (!ok) {
-#pragma unroll
-      for (int j = 0; j < 32; ++j) r[j] = 0u;
-    }
-    if (mok) {
-#pragma unroll
+    const int64_t m = m0 + row;
+    if (m < g.M) {
+      const int64_t lc = mode_offset(l, g.nl, g.l_ext, g.l_sc);
+      const int64_t cm = goff(m, g.nm, g.m_ext, g.m_sc);
+      float* Cp = static_cast<float*>(g.C);
+      const float sx = scalar_as<float>(g.sx), sy = scalar_as<float>(g.sy);
+#pragma unroll 4
       for (int j = 0; j < 32; ++j) {
         const int64_t n = n0 + col + j;
         if (n >= g.N) break;
-        const float v = __uint_as_float(r[j]);
+        const float v = nchunks > 0 ? acc[(col + j) * BM + row] : 0.f;
         if (t.S > 1) {
           t.partial[((split * g.L + l) * g.N + n) * g.M + m] = v;
         } else {
@@ -338,8 +392,14 @@ __global__ void __launch_bounds__(tc::NTHREADS, 1) k_gemm_bf16x3(const __grid_co
     }
   } else if (lane == 0) {
     // ---------------- MMA issue (one thread of the last warp) ----------------
+    // Per K=16 step: t0*t0 into the chunk's main accumulator, the other term
+    // pairs (i + j < NT) into its cross-term accumulator; each chunk starts
+    // both from zero, so TMEM only ever sums CHUNK k-steps.
     const uint32_t sbase = smem_u32(smem);
     for (int kt = 0; kt < nkt; ++kt) {
+      const int c = kt / CHUNK, b = c & 1;
+      const bool first = kt % CHUNK == 0;
+      if (first && c >= 2 && !mbar_wait(&drained[b], (uint32_t)(((c >> 1) - 1) & 1), abort_flag)) break;
       const int s = kt % STAGES;
       if (!mbar_wait(&full[s], (uint32_t)((kt / STAGES) & 1), abort_flag)) break;
       tc_fence_after();
@@ -347,19 +407,30 @@ __global__ void __launch_bounds__(tc::NTHREADS, 1) k_gemm_bf16x3(const __grid_co
 #pragma unroll
       for (int kk = 0; kk < 2; ++kk) {
         const uint32_t off = kk * 256;
-        const uint64_t ah = umma_desc(sb + off), al = umma_desc(sb + TILE_BYTES + off);
-        const uint64_t bh = umma_desc(sb + 2 * TILE_BYTES + off), bl = umma_desc(sb + 3 * TILE_BYTES + off);
-        umma_bf16(tmem, ah, bh, (kt | kk) != 0);
-        umma_bf16(tmem, ah, bl, 1);
-        umma_bf16(tmem, al, bh, 1);
+        uint64_t ad[NT], bd[NT];
+#pragma unroll
+        for (int u = 0; u < NT; ++u) {
+          ad[u] = umma_desc(sb + u * TILE_BYTES + off);
+          bd[u] = umma_desc(sb + (NT + u) * TILE_BYTES + off);
+        }
+        const uint32_t keep = (first && kk == 0) ? 0u : 1u;
+        umma_bf16(tmem_main(b), ad[0], bd[0], keep);
+        bool first_cross = true;
+#pragma unroll
+        for (int d = 1; d < NT; ++d)
+#pragma unroll
+          for (int i = 0; i <= d; ++i) {
+            umma_bf16(tmem_cross(b), ad[i], bd[d - i], first_cross ? keep : 1u);
+            first_cross = false;
+          }
       }
       umma_commit(&empty[s]);
+      if (kt % CHUNK == CHUNK - 1 || kt == nkt - 1) umma_commit(&chunk_done[b]);
     }
-    umma_commit(done);
   }
   tc_fence_before();
   __syncthreads();
-  if (warp == 0) {
+  if (warp == NCONV / 32) {
     tc_fence_after();
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TMEM_COLS) : "memory");
   }
@@ -387,19 +458,23 @@ __global__ void __launch_bounds__(256) k_splitk_reduce(const __grid_constant__ T
   }
 }
 
-bool gemm_bf16x3_supported(const GemmArgs& g) {
+bool gemm_split_supported(const GemmArgs& g) {
   return g.M > 0 && g.N > 0 && g.K > 0 && g.L > 0 && g.M < (1ll << 31) && g.N < (1ll << 31) &&
          (g.M + tc::BM - 1) / tc::BM <= 0x7fffffff && (g.N + tc::BN - 1) / tc::BN <= 65535;
 }
 
-cudaError_t launch_gemm_bf16x3(const GemmArgs& g, void* workspace, size_t ws_bytes, int num_sms, cudaStream_t s) {
+cudaError_t launch_gemm_split(const GemmArgs& g, int nterms, void* workspace, size_t ws_bytes, int num_sms,
+                              cudaStream_t s) {
   using namespace tc;
-  if (!gemm_bf16x3_supported(g)) return cudaErrorNotSupported;
-  static bool attr_set = false;
-  if (!attr_set) {
-    cudaError_t e = cudaFuncSetAttribute(k_gemm_bf16x3, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES);
+  if (!gemm_split_supported(g) || (nterms != 2 && nterms != 3)) return cudaErrorNotSupported;
+  static bool attr_set[2] = {false, false};
+  if (!attr_set[nterms - 2]) {
+    cudaError_t e = nterms == 2 ? cudaFuncSetAttribute(k_gemm_bf16x3<2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                       Cfg<2>::SMEM_BYTES)
+                                : cudaFuncSetAttribute(k_gemm_bf16x3<3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                       Cfg<3>::SMEM_BYTES);
     if (e != cudaSuccess) return e;
-    attr_set = true;
+    attr_set[nterms - 2] = true;
   }
   TcArgs t;
   memset(&t, 0, sizeof(t));
@@ -431,7 +506,8 @@ cudaError_t launch_gemm_bf16x3(const GemmArgs& g, void* workspace, size_t ws_byt
   t.S = (int)S;
   t.kchunk = kchunk;
   dim3 grid((unsigned)tm, (unsigned)tn, (unsigned)(g.L * S));
-  k_gemm_bf16x3<<<grid, NTHREADS, SMEM_BYTES, s>>>(t);
+  if (nterms == 2) k_gemm_bf16x3<2><<<grid, NTHREADS, Cfg<2>::SMEM_BYTES, s>>>(t);
+  else k_gemm_bf16x3<3><<<grid, NTHREADS, Cfg<3>::SMEM_BYTES, s>>>(t);
   count_launch();
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess || S == 1) return e;

@@ -48,12 +48,13 @@ cudaError_t launch_conj(ome_dtype dt, void* x, int64_t n, cudaStream_t s);
 // x <- one(T) over n contiguous elements.
 cudaError_t launch_fill_one(ome_dtype dt, void* x, int64_t n, cudaStream_t s);
 
-// Tensor-core FP32 GEMM from BF16x3 split products (tcgen05 + TMEM).
-// Returns cudaErrorNotSupported when the shape/strides are outside the
-// kernel's preconditions (the caller then uses the CUDA-core kernel).
-cudaError_t launch_gemm_bf16x3(const GemmArgs& g, void* workspace, size_t ws_bytes, int num_sms,
-                               cudaStream_t s);
-bool gemm_bf16x3_supported(const GemmArgs& g);
+// Tensor-core FP32 GEMM from BF16 split products (tcgen05 + TMEM): nterms = 2
+// (BF16x3, 3 MMAs per K step) or 3 (BF16x6, 6 MMAs, FP32-faithful).
+// Returns cudaErrorNotSupported when the shape is outside the kernel's
+// preconditions (the caller then uses the CUDA-core kernel).
+cudaError_t launch_gemm_split(const GemmArgs& g, int nterms, void* workspace, size_t ws_bytes, int num_sms,
+                              cudaStream_t s);
+bool gemm_split_supported(const GemmArgs& g);
 
 // Synchronise s and read/clear the device timeout flag: 1 if a bounded wait
 // gave up, 0 if not, -cudaError on failure.

@@ -125,6 +125,53 @@ std::vector<int32_t> child_labels(const ome_plan* p, int ref, bool sliced) {
   return r;
 }
 
+// Memory order of intermediates.  An intermediate's label order is internal to
+// the plan (only the root's is the caller's), so each binary node lays out its
+// children for itself, as analyze_binary's canonical orders do
+// (src/einsum.jl:139-185; OMEinsumContractionOrders' optimize_permute):
+// x1 = [outer1 (output order), inner, batch (output order)],
+// x2 = [inner, outer2 (output order), batch (output order)], with one inner
+// order shared by both (a leaf child's, if either child is a leaf).  Mode
+// groups of the strided GEMM then merge into one or a few modes.  Top-down:
+// a parent's order is final before its children are arranged.
+void canonical_orders(ome_plan* p) {
+  const int nn = (int)p->nodes.size();
+  for (int j = nn - 1; j >= 0; --j) {
+    PNode& n = p->nodes[j];
+    if (n.args.size() != 2) continue;
+    const int r1 = n.args[0], r2 = n.args[1];
+    const std::vector<int32_t> L1 = r1 >= 0 ? p->nodes[r1].iy : p->in_labels[-r1 - 1];
+    const std::vector<int32_t> L2 = r2 >= 0 ? p->nodes[r2].iy : p->in_labels[-r2 - 1];
+    const std::vector<int32_t>& y = n.iy;
+    std::vector<int32_t> o1, o2, batch, inner, d1, d2;
+    for (int32_t l : y) {
+      const bool a = contains(L1, l), b = contains(L2, l);
+      if (a && b) batch.push_back(l);
+      else if (a) o1.push_back(l);
+      else if (b) o2.push_back(l);
+    }
+    const std::vector<int32_t>& ref = (r1 < 0 || r2 >= 0) ? L1 : L2;  // a leaf's order if there is one
+    for (int32_t l : ref)
+      if (contains(L1, l) && contains(L2, l) && !contains(y, l)) inner.push_back(l);
+    for (int32_t l : L1)
+      if (!contains(L2, l) && !contains(y, l)) d1.push_back(l);
+    for (int32_t l : L2)
+      if (!contains(L1, l) && !contains(y, l)) d2.push_back(l);
+    auto rebuild = [&](int r, const std::vector<std::vector<int32_t>>& parts) {
+      std::vector<int32_t> v;
+      for (auto& q : parts) v.insert(v.end(), q.begin(), q.end());
+      PNode& c = p->nodes[r];
+      if (v.size() != c.iy.size()) return;  // not a permutation of the child's labels: keep
+      c.iy = v;
+      c.iy_s.clear();
+      for (int32_t l : v)
+        if (!contains(p->sliced, l)) c.iy_s.push_back(l);
+    };
+    if (r1 >= 0) rebuild(r1, {o1, inner, batch, d1});
+    if (r2 >= 0) rebuild(r2, {inner, o2, batch, d2});
+  }
+}
+
 }  // namespace
 
 extern "C" {
@@ -209,6 +256,7 @@ int ome_plan_create(ome_ctx* ctx, ome_dtype dtype, int32_t ninputs, const int32_
     for (int32_t l : n.iy) n.numel *= p->ext[l];
     for (int32_t l : n.iy_s) n.numel_s *= p->ext[l];
   }
+  canonical_orders(p);
   for (int t = 0; t < ninputs; ++t)
     if (!input_used[t]) {
       delete p;
@@ -219,22 +267,23 @@ int ome_plan_create(ome_ctx* ctx, ome_dtype dtype, int32_t ninputs, const int32_
       delete p;
       return set_err(OME_INVALID_ARGUMENT, "node %d is not reachable from the root", j);
     }
-  // forward arena (sliced shapes), liveness: a node's output dies when its parent ran
+  // forward arena (sliced shapes), liveness: a node's output dies when its
+  // parent ran.  The FP64 cross-slice accumulator lives through every slice,
+  // so it is reserved first and never shared with a node buffer.
   const int root = nnodes - 1;
+  const bool sliced = !p->sliced.empty();
+  p->acc64 = sliced && (dtype == OME_F32 || dtype == OME_F64 || dtype == OME_C32);
   Arena ar;
+  if (p->acc64) p->acc_off = ar.alloc((size_t)p->nodes[root].numel * (dtype == OME_C32 ? 16 : 8));
   for (int j = 0; j < root; ++j) {
     PNode& n = p->nodes[j];
     n.off_fwd = ar.alloc((size_t)n.numel_s * p->esize);
     for (int r : n.args)
       if (r >= 0) ar.release(p->nodes[r].off_fwd);
   }
-  const bool sliced = !p->sliced.empty();
-  p->acc64 = sliced && (dtype == OME_F32 || dtype == OME_F64 || dtype == OME_C32);
-  if (p->acc64) {
-    // keep root children alive while the temporary and accumulator exist
-    p->tmp_off = ar.alloc((size_t)p->nodes[root].numel_s * p->esize);
-    p->acc_off = ar.alloc((size_t)p->nodes[root].numel * (dtype == OME_C32 ? 16 : 8));
-  }
+  // the root's temporary is written after every other node of the slice ran
+  // (its children are still live here, so it cannot overlap them)
+  if (p->acc64) p->tmp_off = ar.alloc((size_t)p->nodes[root].numel_s * p->esize);
   p->arena_bytes = ar.peak;
   // per-node dispatch scratch: dangling-label reductions (bounded by the
   // children's sizes), split-reduction partials and GEMM workspace

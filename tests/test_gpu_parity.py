@@ -129,15 +129,18 @@ def test_gemm_shapes(code, sizes, dt):
         assert_match(got, oracle(ixs, iy, xs, sizes, dt, wide=True), dt)
 
 
-def test_plain_fp32_path_matches():
+@pytest.mark.parametrize("prec,rtol", [(1, 1e-6), (2, 1e-5), (3, 1e-6)])
+def test_precision_modes(prec, rtol):
+    """FP32 (CUDA cores), BF16x3 and BF16x6 (tensor cores) against FP64."""
     rng = np.random.default_rng(5)
-    a, b = rng.standard_normal((200, 300)).astype(np.float32), rng.standard_normal((300, 100)).astype(np.float32)
-    ome.set_einsum_backend(ome.B200Backend(prec=1))
+    a, b = rng.standard_normal((200, 3000)).astype(np.float32), rng.standard_normal((3000, 300)).astype(np.float32)
+    ome.set_einsum_backend(ome.B200Backend(prec=prec))
     try:
         got = to_np(ome.ein("ij,jk->ik")(to_dev(a, "f32"), to_dev(b, "f32")))
+        ome.device_status()
     finally:
         ome.set_einsum_backend(ome.B200Backend())
-    assert_match(got, a.astype(np.float64) @ b.astype(np.float64), "f32")
+    assert_match(got, a.astype(np.float64) @ b.astype(np.float64), "f32", rtol)
 
 
 def test_loop_einsum_entry():

@@ -120,3 +120,32 @@ def test_three_colouring_petersen_int64():
     code = ome.ein("afl,bhn,cjf,dlh,enj,ago,big,cki,dmk,eom->")
     opt = ome.optimize_code(code, ome.uniformsize(code, 3), ome.GreedyMethod())
     assert int(opt(*([sd] * 10))) == 0
+
+
+@pytest.mark.parametrize("dt", ["f64", "f32", "i64"])
+def test_sliced_network_many_nodes(dt):
+    """A 3-regular network (24 vertices, bond 2) sliced on three labels equals
+    the unsliced tree; exercises the workspace plan with many live buffers."""
+    rng = np.random.default_rng(12)
+    n = 24
+    while True:
+        stubs = np.repeat(np.arange(n), 3)
+        rng.shuffle(stubs)
+        pairs = [tuple(sorted(p)) for p in stubs.reshape(-1, 2)]
+        if all(a != b for a, b in pairs) and len(set(pairs)) == len(pairs):
+            break
+    inc = [[] for _ in range(n)]
+    for i, (a, b) in enumerate(pairs):
+        inc[a].append(i)
+        inc[b].append(i)
+    code = ome.EinCode([tuple(v) for v in inc], ())
+    sd = {i: 2 for i in range(len(pairs))}
+    opt = ome.optimize_code(code, sd, ome.GreedyMethod(nrepeat=2))
+    inner = [l for l in ome.label_elimination_order(opt)][:3]
+    se = ome.SlicedEinsum(inner, opt)
+    xs = [gen(rng, (2, 2, 2), dt) for _ in range(n)]
+    want = O.nested_einsum(oracle_tree(opt), xs, sd)
+    got = to_np(se(*[to_dev(x, dt) for x in xs]))
+    assert_match(got, want, dt, 1e-5 if dt == "f32" else None)
+    got2 = to_np(opt(*[to_dev(x, dt) for x in xs]))
+    assert_match(got2, want, dt, 1e-5 if dt == "f32" else None)
