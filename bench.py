@@ -139,7 +139,7 @@ class ClockSampler:
         if not sm:
             return None
         return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
-                "samples": len(sm)}
+                "samples": len(sm), "window": "from 1 s of warm-up load through the timed steps"}
 
 
 def cpu_suite(O, inputs, steps=1):
@@ -150,6 +150,197 @@ def cpu_suite(O, inputs, steps=1):
             ixs, iy = parse_code(code)
             O.einsum(ixs, iy, xs, ext)
     return (time.perf_counter() - t0) / steps
+
+
+def run_case_only(ome, name, dev):
+    """Run one suite contraction twice (warm-up + the launch a profiler captures)."""
+    import torch
+    for nm, code, ext, seed in CASES:
+        if nm != name:
+            continue
+        xs = [torch.from_numpy(x).to(dev) for x in make_inputs(code, ext, seed)]
+        ixs, iy = parse_code(code)
+        c = ome.EinCode(ixs, iy)
+        y = ome.get_output_array(xs, [ext[l] for l in iy])
+        for _ in range(2):
+            ome.einsum_(c, xs, y, True, False, ext)
+        torch.cuda.synchronize()
+        ome.device_status()
+        return
+    raise SystemExit(f"unknown case {name!r}; one of {[c[0] for c in CASES]}")
+
+
+def random_regular3(n, seed):
+    """Random 3-regular graph (pairing model, resampled until simple), numpy seed."""
+    rng = np.random.default_rng(seed)
+    while True:
+        stubs = np.repeat(np.arange(n), 3)
+        rng.shuffle(stubs)
+        pairs = stubs.reshape(-1, 2)
+        if np.any(pairs[:, 0] == pairs[:, 1]):
+            continue
+        e = set()
+        ok = True
+        for a, b in pairs:
+            k = (int(min(a, b)), int(max(a, b)))
+            if k in e:
+                ok = False
+                break
+            e.add(k)
+        if ok:
+            return sorted(e)
+
+
+def tn_network(ome, n, graph_seed=7, value_seed=8, scale=True):
+    """3-regular tensor network: one rank-3 bond-2 tensor per vertex, labels =
+    edges; FP32 normal(0,1)/sqrt(3) entries (unscaled if scale=False)."""
+    import math
+    edges = random_regular3(n, graph_seed)
+    inc = [[] for _ in range(n)]
+    for i, (a, b) in enumerate(edges):
+        inc[a].append(i)
+        inc[b].append(i)
+    code = ome.EinCode([tuple(v) for v in inc], ())
+    sd = {i: 2 for i in range(len(edges))}
+    rng = np.random.default_rng(value_seed)
+    f = 1 / math.sqrt(3) if scale else 1.0
+    xs = [(rng.standard_normal((2, 2, 2)) * f).astype(np.float32) for _ in range(n)]
+    return code, sd, xs
+
+
+def tn_section(ome, dev, n=180, sc_target=27):
+    """Precision and speed of a 3-regular n=180 network: plain FP32 (CUDA
+    cores) vs BF16x6 / BF16x3 (tensor cores), each against FP64 on the same
+    plan, FP64 cross-slice sums."""
+    import torch
+    code, sd, xs = tn_network(ome, n)
+    opt = ome.optimize_code(code, sd, ome.GreedyMethod(nrepeat=10, seed=0))
+    se = ome.slice_code(opt, sd, ome.GreedySlicer(sc_target=sc_target))
+    cs = ome.contraction_complexity(se, sd)
+    out = {"workload": f"random 3-regular graph n={n} (seed 7), bond 2, FP32 normal(0,1)/sqrt(3) (seed 8); "
+                       f"greedy order (seed 0), sliced to 2^{sc_target} elements "
+                       f"({len(se.slicing)} labels, {2 ** len(se.slicing)} slices), tc=2^{cs.tc:.2f}",
+           "flops_per_contraction": 2 * 2 ** cs.tc}
+    vals = {}
+    for name, dt, prec in [("fp64", torch.float64, 0), ("fp32", torch.float32, 1), ("bf16x6", torch.float32, 3),
+                           ("bf16x3", torch.float32, 2)]:
+        ome.set_einsum_backend(ome.B200Backend(prec=prec))
+        d = [torch.from_numpy(x.astype(np.float64 if dt == torch.float64 else np.float32)).to(dev) for x in xs]
+        r = se(*d)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        r = se(*d)
+        e1.record()
+        torch.cuda.synchronize()
+        ome.device_status()
+        vals[name] = float(r.double().cpu())
+        out[name] = {"s": e0.elapsed_time(e1) / 1e3, "value": vals[name]}
+    for k in ("fp32", "bf16x6", "bf16x3"):
+        out[k]["rel_err_vs_fp64"] = abs(vals[k] - vals["fp64"]) / abs(vals["fp64"])
+        out[k]["contractions_per_s"] = 1.0 / out[k]["s"]
+    out["speedup_bf16x6_vs_fp32"] = out["fp32"]["s"] / out["bf16x6"]["s"]
+    ome.set_einsum_backend(ome.B200Backend())
+    return out
+
+
+def mps_jobs(njobs, seed):
+    rng = np.random.default_rng(seed)
+    jobs = []
+    for _ in range(njobs):
+        a, b, d, e = (int(8 * rng.integers(1, 17)) for _ in range(4))
+        jobs.append(dict(a=a, b=b, c=int(rng.choice([2, 4])), d=d, e=e))
+    return jobs
+
+
+def batch_section(ome, dev, njobs=8192, seed=9):
+    """8192 MPS transfer contractions ein"(ab,bcd),de->ace" (ComplexF32, bond
+    dims in {8,...,128}, c in {2,4}): two grouped launches in a CUDA graph vs
+    one launch per contraction (host loop, and the same launches in a graph)."""
+    import torch
+    jobs = mps_jobs(njobs, seed)
+    g = torch.Generator(device=dev).manual_seed(seed)
+    def cx(*shape):  # column-major (Julia layout) ComplexF32 normal(0,1) re/im
+        r = torch.randn(*shape[::-1], generator=g, device=dev)
+        i = torch.randn(*shape[::-1], generator=g, device=dev)
+        return torch.complex(r, i).permute(*range(len(shape) - 1, -1, -1))
+    X = [(cx(j["a"], j["b"]), cx(j["b"], j["c"], j["d"]), cx(j["d"], j["e"])) for j in jobs]
+    flops = sum(8 * (j["a"] * j["b"] * j["c"] * j["d"] + j["a"] * j["c"] * j["d"] * j["e"]) for j in jobs)
+    code1, code2 = ome.ein("ab,bcd->acd"), ome.ein("acd,de->ace")
+    b1 = ome.BatchedEinsum(code1, [(x[0], x[1]) for x in X])
+    b2 = ome.BatchedEinsum(code2, [(t, x[2]) for t, x in zip(b1.outputs, X)])
+    graph = ome.capture_graph(lambda: (b1.run(), b2.run()))
+
+    def timed(fn, reps=3):
+        fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(reps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps
+
+    t_group = timed(graph.replay)
+    mids = [torch.empty_like(t) for t in b1.outputs]
+    outs = [torch.empty_like(t) for t in b2.outputs]
+    sd = [dict(j) for j in jobs]
+
+    def per_contraction():
+        for j, x, m, o in zip(sd, X, mids, outs):
+            ome.einsum_(code1, [x[0], x[1]], m, True, False, j)
+            ome.einsum_(code2, [m, x[2]], o, True, False, j)
+
+    t_loop = timed(per_contraction, reps=1)
+    graph2 = ome.capture_graph(per_contraction)
+    t_loop_graph = timed(graph2.replay)
+    err = max(float((a - b).abs().max() / b.abs().max()) for a, b in zip(outs[:64], b2.outputs[:64]))
+    return {"workload": f"{njobs} MPS transfer contractions (ab,bcd),de->ace, a,b,d,e uniform in "
+                        "{8,16,...,128}, c in {2,4}, ComplexF32 normal(0,1) re/im (seed 9)",
+            "contractions": 2 * njobs, "complex_flops": flops,
+            "grouped_graph_ms": t_group, "per_contraction_loop_ms": t_loop,
+            "per_contraction_graph_ms": t_loop_graph,
+            "jobs_per_s_grouped": njobs / (t_group / 1e3), "jobs_per_s_loop": njobs / (t_loop / 1e3),
+            "speedup_vs_loop": t_loop / t_group, "speedup_vs_graphed_loop": t_loop_graph / t_group,
+            "tflops_grouped": flops / (t_group / 1e3) / 1e12,
+            "tile_config": [b1.tile_config, b2.tile_config], "autotune_us": [b1.tuned_us, b2.tuned_us],
+            "max_rel_diff_grouped_vs_loop": err}
+
+
+def serve_section(ome, dev, njobs=32, rate=2000.0, seed=10, nmin=40, nmax=200, grad_frac=0.1, cap_s=90.0):
+    """Serving: Poisson arrivals (rate/s) of whole 3-regular networks, n uniform
+    over even [nmin, nmax], bond 2, unscaled FP32 normal(0,1) entries (power-of-
+    two rescaled, log2 scale in FP64), 10% cost_and_gradient jobs; admitted by
+    planned peak workspace bytes; 16 slots share a 150 GB budget."""
+    import torch
+    rng = np.random.default_rng(seed)
+    t = np.cumsum(rng.exponential(1.0 / rate, njobs))
+    ns = rng.integers(nmin // 2, nmax // 2 + 1, njobs) * 2
+    grads = rng.random(njobs) < grad_frac
+    jobs, plan_s = [], 0.0
+    for i, (n, g) in enumerate(zip(ns, grads)):
+        code, sd, xs = tn_network(ome, int(n), graph_seed=1000 + i, value_seed=2000 + i, scale=False)
+        t0 = time.perf_counter()
+        opt = ome.optimize_code(code, sd, ome.GreedyMethod(nrepeat=1, seed=i))
+        if ome.contraction_complexity(opt, sd).sc > 27 and not g:
+            opt = ome.slice_code(opt, sd, ome.GreedySlicer(sc_target=27))
+        plan_s += time.perf_counter() - t0
+        xs, exps = ome.pow2_rescale(xs)
+        jobs.append(ome.Job(opt, [torch.from_numpy(x).to(dev) for x in xs], grad=bool(g), arrival=float(t[i]),
+                            log2_scale=float(sum(exps))))
+    ome.release_workspaces()
+    torch.cuda.empty_cache()
+    srv = ome.TNServer(n_slots=16, hbm_budget_bytes=150e9)
+    st = srv.run_trace(jobs, timeout_s=cap_s)
+    srv.close()
+    done = [j for j in jobs if j.done >= 0 and j.value is not None and j in srv.finished]
+    st.update({"workload": f"{njobs} jobs, Poisson {rate:.0f}/s (seed {seed}), n uniform even [{nmin},{nmax}], "
+                           "bond 2, unscaled FP32 normal(0,1), 10% gradient jobs, greedy order + slicing to 2^27 "
+                           "(client side), 16 slots sharing a 150 GB workspace budget",
+               "submitted": njobs, "incomplete": njobs - len(done), "cap_s": cap_s,
+               "client_planning_s": plan_s, "n_of_completed": sorted(int(len(j.xs)) for j in done)})
+    return st
 
 
 def run_reference(args, rank):
@@ -182,6 +373,11 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--prec", type=int, default=0, help="0 AUTO (BF16x3), 1 plain FP32")
     ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline leg")
+    ap.add_argument("--no-tn", action="store_true", help="skip the tensor-network precision section")
+    ap.add_argument("--no-batch", action="store_true", help="skip the batched MPS-transfer section")
+    ap.add_argument("--no-serve", action="store_true", help="skip the serving section")
+    ap.add_argument("--case", default=None,
+                    help="profiling aid: run only this suite contraction (e.g. 'ijk->j') twice and exit")
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -202,6 +398,8 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     ome.set_einsum_backend(ome.B200Backend(prec=args.prec))
     lib = ome.load_library()
+    if args.case is not None:
+        return run_case_only(ome, args.case, dev)
 
     hosts, devs, outs, codes = [], [], [], []
     for name, code, ext, seed in CASES:
@@ -225,18 +423,24 @@ def main():
             if k is not None:
                 ev[k][i][1].record()
 
-    for _ in range(max(args.warmup, 3)):
+    cs = ClockSampler(local).__enter__()   # sampling starts under the warm-up load
+    t_w = time.perf_counter()
+    nw = 0
+    while nw < max(args.warmup, 3) or time.perf_counter() - t_w < 1.0:
         step()
+        nw += 1
+        if nw % 8 == 0:
+            torch.cuda.synchronize()
     torch.cuda.synchronize()
     if world > 1:
         dist.barrier()
     n0 = lib.ome_launch_count()
-    with ClockSampler(local) as cs:
-        torch.cuda.synchronize()
-        for k in range(args.steps):
-            step(k)
-        torch.cuda.synchronize()
+    torch.cuda.synchronize()
+    for k in range(args.steps):
+        step(k)
+    torch.cuda.synchronize()
     launches = lib.ome_launch_count() - n0
+    cs.__exit__()
     if world > 1:
         dist.barrier()
     per_case = [sum(ev[k][i][0].elapsed_time(ev[k][i][1]) for k in range(args.steps)) / args.steps
@@ -275,14 +479,15 @@ def main():
     name, code, ext, _ = CASES[dom]
     flops, nbytes = case_work(code, ext)
     dur_s = per_case[dom] / 1e3
-    tc_peak = bf16 / 3.0  # BF16x3: three BF16 products per FP32 product
+    nmma = {0: 6, 3: 6, 2: 3}.get(args.prec, 6)   # BF16 MMAs per FP32 product (BF16x6 / BF16x3)
+    tc_peak = bf16 / nmma
     t_flop = flops / (tc_peak * 1e12) if flops else 0.0
     t_mem = nbytes / (hbm * 1e9)
     traffic = load_traffic().get(name)
     if t_flop > t_mem:
         roof = {"bound": "tensor", "achieved": flops / dur_s / 1e12, "peak": tc_peak, "unit": "TFLOP/s",
                 "frac": (flops / dur_s / 1e12) / tc_peak, "traffic": traffic,
-                "kernel": name, "peak_source": f"{src} bf16_tflops / 3 (FP32-equivalent BF16x3)"}
+                "kernel": name, "peak_source": f"{src} bf16_tflops / {nmma} (FP32-equivalent of BF16x{nmma})"}
     else:
         roof = {"bound": "hbm", "achieved": nbytes / dur_s / 1e9, "peak": hbm, "unit": "GB/s",
                 "frac": (nbytes / dur_s / 1e9) / hbm, "traffic": traffic, "kernel": name,
@@ -298,6 +503,14 @@ def main():
                "sample": "the full suite once, NumPy/OpenBLAS DefaultBackend restatement "
                          f"(BLAS threads = {os.cpu_count()}; copies single-threaded)"}
 
+    del devs, outs, flush
+    ome.release_workspaces()
+    torch.cuda.empty_cache()
+    tn = None if (args.no_tn or world > 1) else tn_section(ome, dev)
+    ome.release_workspaces()
+    torch.cuda.empty_cache()
+    batch = None if (args.no_batch or world > 1) else batch_section(ome, dev)
+    serve = None if (args.no_serve or world > 1) else serve_section(ome, dev)
     detail = {}
     for (nm, code, ext, _), ms in zip(CASES, per_case):
         f, b = case_work(code, ext)
@@ -306,15 +519,17 @@ def main():
             detail[nm]["TFLOP/s"] = f / (ms / 1e3) / 1e12
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": "contractions/s", "n_gpus": world, "steps": args.steps,
-                "warmup": max(args.warmup, 3), "ms_per_step": step_ms_max, "higher_is_better": True,
+                "warmup": nw, "ms_per_step": step_ms_max, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded normal(0,1))",
                 "config": {"workload": WORKLOAD, "l2": "flushed by a 256 MiB write before every contraction",
-                           "prec": "BF16x3 where GEMM-shaped" if args.prec == 0 else "plain FP32",
+                           "prec": {0: "BF16x6 tensor-core split products (FP32-faithful) where GEMM-shaped",
+                                    1: "plain FP32 (CUDA cores)", 2: "BF16x3 where GEMM-shaped",
+                                    3: "BF16x6 where GEMM-shaped"}[args.prec],
                            "parallelism": f"replicas x{world}", "per_case": detail},
                 "e2e": {"value": e2e_value, "unit": "contractions/s", "h2d_bytes_per_step": h2d,
                         "d2h_bytes_per_step": d2h},
                 "gpu_launches": int(launches), "roofline": roof, "cpu_baseline": cpu,
-                "clocks": cs.summary()}
+                "clocks": cs.summary(), "tn_precision": tn, "batching": batch, "serving": serve}
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.destroy_process_group()

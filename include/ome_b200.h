@@ -172,6 +172,25 @@ OME_API int ome_plan_gradient(ome_ctx* ctx, ome_plan* plan, void* stream,
                       const void* const* inputs, const void* dy, void* y,
                       void* const* dxs);
 
+/* Batched contractions of uneven shapes (one grouped launch) ----------------
+ *
+ * `count` binary einsums y_i <- sy*y_i + sx*f(x1_i, x2_i) whose label groups
+ * (outer1, outer2, inner, batch) each merge into one strided mode -- e.g.
+ * every contraction of an MPS sweep.  ome_batch_create analyses them like
+ * ome_einsum does (src/einsum.jl:139-211), uploads a problem table, and times
+ * the candidate tile shapes on the batch (tile_config < 0; or pick 0..2);
+ * ome_batch_run issues ONE persistent grouped kernel over all problems' tiles
+ * (capturable in a CUDA graph).  Tensors are bound at creation: the buffers
+ * must stay valid.  Replaces a loop of einsum! calls, one launch each. */
+typedef struct ome_batch ome_batch;
+OME_API int ome_batch_create(ome_ctx* ctx, void* stream, ome_dtype dtype, int32_t count,
+                             const ome_tensor* x1s, const ome_tensor* x2s, const ome_tensor* ys,
+                             int32_t tile_config, ome_batch** out);
+OME_API int ome_batch_run(ome_ctx* ctx, ome_batch* batch, void* stream, const void* sx, const void* sy);
+/* Chosen tile shape (0: 32x32, 1: 64x32, 2: 64x64) and the autotuner's timings (us, 3 floats). */
+OME_API int ome_batch_info(const ome_batch* batch, int32_t* tile_config, float* tuned_us);
+OME_API int ome_batch_destroy(ome_batch* batch);
+
 /* Allocation-free reduction --------------------------------------------------
  *
  * No counterpart in the reference.  y <- sy*y + sx*sum(x) where every label

@@ -15,12 +15,16 @@ Public API (names follow OMEinsum.jl; ``!`` becomes a trailing ``_``):
 * planning: ``optimize_code``, ``slice_code``, ``GreedyMethod``,
   ``GreedySlicer``, ``contraction_complexity``, ``flop``, ``peak_memory``,
   ``label_elimination_order``, ``writejson``, ``readjson``;
+* batching: ``BatchedEinsum`` (one grouped launch for many contractions of
+  uneven shapes), ``capture_graph``;
+* serving: ``TNServer`` / ``Job`` (continuous batching of whole networks by
+  peak workspace bytes, p50/p99 latency);
 * element types: torch float32/float64/complex64/complex128/int64/bool and
   ``TropicalTensor`` (max-plus).
 
 Every contraction runs in libomeb200.so; there is no CPU fallback.
 """
-from ._lib import ArgumentError, DimensionMismatch, OMEError, device_status, load as load_library
+from ._lib import ArgumentError, DimensionMismatch, OMEError, device_status, load as load_library, release_workspaces
 from .backends import (B200Backend, CuTensorBackend, DefaultBackend, EinsumBackend, get_einsum_backend,
                        set_einsum_backend)
 from .core import (AbstractEinsum, DynamicEinCode, DynamicNestedEinsum, EinCode, NestedEinsum, SlicedEinsum,
@@ -28,6 +32,8 @@ from .core import (AbstractEinsum, DynamicEinCode, DynamicNestedEinsum, EinCode,
                    parse_nested, slice_iterator, uniformsize)
 from .engine import (TropicalTensor, cost_and_gradient, einsum, einsum_, einsum_grad, get_output_array,
                      loop_einsum, loop_einsum_, promote_dtype)
+from .batch import BatchedEinsum, capture_graph
+from .serve import Job, TNServer, pow2_rescale
 from .planner import (GreedyMethod, GreedySlicer, contraction_complexity, flop, label_elimination_order,
                       optimize_code, peak_memory, readjson, slice_code, writejson)
 

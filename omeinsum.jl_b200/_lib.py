@@ -22,7 +22,8 @@ PREC_AUTO, PREC_FP32, PREC_BF16X3, PREC_BF16X6 = range(4)
 EXPORTS = [
     "ome_version", "ome_launch_count", "ome_device_status", "ome_last_error", "ome_ctx_create", "ome_ctx_destroy", "ome_ctx_workspace_bytes",
     "ome_einsum", "ome_loop_einsum", "ome_plan_create", "ome_plan_destroy", "ome_plan_peak_bytes",
-    "ome_plan_execute", "ome_plan_gradient", "ome_reduce_noalloc",
+    "ome_plan_execute", "ome_plan_gradient", "ome_reduce_noalloc", "ome_batch_create", "ome_batch_run",
+    "ome_batch_info", "ome_batch_destroy",
 ]
 
 
@@ -83,6 +84,11 @@ def load() -> C.CDLL:
         lib.ome_plan_peak_bytes.argtypes = [P, C.POINTER(C.c_size_t), C.POINTER(C.c_size_t)]
         lib.ome_plan_execute.argtypes = [P, P, P, C.POINTER(P), P, P, P]
         lib.ome_plan_gradient.argtypes = [P, P, P, C.POINTER(P), P, P, C.POINTER(P)]
+        lib.ome_batch_create.argtypes = [P, P, C.c_int, C.c_int32, C.POINTER(Tensor), C.POINTER(Tensor),
+                                         C.POINTER(Tensor), C.c_int32, C.POINTER(P)]
+        lib.ome_batch_run.argtypes = [P, P, P, P, P]
+        lib.ome_batch_info.argtypes = [P, C.POINTER(C.c_int32), C.POINTER(C.c_float)]
+        lib.ome_batch_destroy.argtypes = [P]
         lib.ome_reduce_noalloc.argtypes = [P, C.c_int, C.POINTER(Tensor), C.POINTER(Tensor), P, P]
         for f in EXPORTS:
             if f not in ("ome_version", "ome_last_error", "ome_launch_count"):
@@ -133,6 +139,16 @@ class Context:
 
 
 _contexts: dict[int, Context] = {}
+
+
+def release_workspaces() -> None:
+    """Destroy the per-device contexts (their workspaces); they are re-created on demand."""
+    import torch
+
+    for d, c in list(_contexts.items()):
+        torch.cuda.synchronize(d)
+        c.close()
+        del _contexts[d]
 DEFAULT_WORKSPACE = 256 << 20
 
 

@@ -286,19 +286,27 @@ int ome_plan_create(ome_ctx* ctx, ome_dtype dtype, int32_t ninputs, const int32_
   if (p->acc64) p->tmp_off = ar.alloc((size_t)p->nodes[root].numel_s * p->esize);
   p->arena_bytes = ar.peak;
   // per-node dispatch scratch: dangling-label reductions (bounded by the
-  // children's sizes), split-reduction partials and GEMM workspace
-  size_t scratch = 0;
-  for (int j = 0; j < nnodes; ++j) {
-    size_t sj = 0;
-    for (int r : p->nodes[j].args) {
-      int64_t c = 1;
-      if (r >= 0) c = p->nodes[r].numel;
-      else for (int32_t l : p->in_labels[-r - 1]) c *= p->ext[l];
-      sj += ((size_t)c * p->esize + 255) & ~(size_t)255;
+  // children's sizes), split-reduction partials and GEMM workspace; sliced
+  // sizes for the forward plan, full sizes for the (unsliced) gradient
+  auto scratch_bound = [&](bool use_sliced) {
+    size_t scratch = 0;
+    for (int j = 0; j < nnodes; ++j) {
+      size_t sj = 0;
+      for (int r : p->nodes[j].args) {
+        int64_t c = 1;
+        if (r >= 0) {
+          c = use_sliced ? p->nodes[r].numel_s : p->nodes[r].numel;
+        } else {
+          for (int32_t l : p->in_labels[-r - 1])
+            if (!(use_sliced && contains(p->sliced, l))) c *= p->ext[l];
+        }
+        sj += ((size_t)c * p->esize + 255) & ~(size_t)255;
+      }
+      scratch = std::max(scratch, sj);
     }
-    scratch = std::max(scratch, sj);
-  }
-  scratch += (size_t)64 << 20;
+    return scratch + ((size_t)64 << 20);
+  };
+  const size_t scratch = scratch_bound(true), scratch_grad = scratch_bound(false);
   p->fwd_bytes = ((p->arena_bytes + 255) & ~(size_t)255) + scratch;
   // gradient arena: all forward values kept (unsliced) plus one gradient each
   size_t g = 0;
@@ -314,7 +322,7 @@ int ome_plan_create(ome_ctx* ctx, ome_dtype dtype, int32_t ninputs, const int32_
   }
   p->dy_off = g;
   p->grad_arena = g + ((size_t)p->nodes[root].numel * p->esize + 511);
-  p->grad_bytes = ((p->grad_arena + 255) & ~(size_t)255) + scratch;
+  p->grad_bytes = ((p->grad_arena + 255) & ~(size_t)255) + scratch_grad;
   *out = p;
   return OME_OK;
 }
