@@ -308,7 +308,7 @@ static int run_loop(ome_ctx* ctx, cudaStream_t s, ome_dtype dt, int nin, const H
     for (int m = 0; m < outer.n && vec; ++m) vec = (outer.str[1][m] * (int64_t)es) % 16 == 0;
     if (inner.n == 2) vec = vec && (inner.str[1][1] * (int64_t)es) % 16 == 0;
     int64_t nsplit = 1;
-    const int64_t target = (int64_t)sms * 8;
+    const int64_t target = (int64_t)sms * 16;
     if (n_out < target) nsplit = std::min<int64_t>((target + n_out - 1) / n_out, R);
     int64_t rchunk = (R + nsplit - 1) / nsplit;
     nsplit = (R + rchunk - 1) / rchunk;

@@ -240,6 +240,25 @@ struct LoopArgs {
 
 // Permute / broadcast copy: y[modes] <- sx*x[modes] (+ sy*y).  Mode 0 is y's
 // fastest mode; tmode (>0) is x's fastest mode for the tiled transpose, or -1.
+// Division of n < 2^31 by an invariant d >= 1 with one multiply-high, add and
+// shift (Granlund & Montgomery, "Division by invariant integers using
+// multiplication", PLDI 1994, round-up multiplier m = floor(2^32 (2^l - d) / d) + 1,
+// l = ceil(log2 d)).  (umulhi(n, m) + n) stays below 2^32 for n < 2^31.
+struct FastDiv {
+  uint32_t d, m, l;
+};
+
+static inline FastDiv make_fastdiv(uint32_t d) {
+  uint32_t l = 0;
+  while (l < 32 && ((uint64_t)1 << l) < d) ++l;
+  const uint64_t m = (((uint64_t)1 << 32) * (((uint64_t)1 << l) - d)) / d + 1;
+  return FastDiv{d, (uint32_t)m, l};
+}
+
+__device__ __forceinline__ uint32_t fast_div(uint32_t n, const FastDiv& f) {
+  return (__umulhi(n, f.m) + n) >> f.l;
+}
+
 struct PermArgs {
   const void* x;
   void* y;

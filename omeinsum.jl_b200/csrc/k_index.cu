@@ -12,6 +12,13 @@
 
 namespace ome {
 
+// Largest |offset| reachable over the modes (sum of (ext-1)*|stride|).
+static int64_t max_offset(int nd, const int64_t* ext, const int64_t* str) {
+  int64_t m = 0;
+  for (int i = 0; i < nd; ++i) m += (ext[i] > 0 ? ext[i] - 1 : 0) * (str[i] < 0 ? -str[i] : str[i]);
+  return m;
+}
+
 static unsigned long long g_launches = 0;
 unsigned long long launch_counter() { return __atomic_load_n(&g_launches, __ATOMIC_RELAXED); }
 void count_launch(int n) { __atomic_fetch_add(&g_launches, (unsigned long long)n, __ATOMIC_RELAXED); }
@@ -216,11 +223,12 @@ __global__ void __launch_bounds__(256) k_loop_finish(const __grid_constant__ Loo
 // elements x R rows (at most one more summed mode, row stride rs).  One block
 // per (output, row split); 16-byte vector loads when VEC (every row start
 // 16-byte aligned and E0 a multiple of the vector width), 4 loads in flight.
-template <class A, bool VEC>
-__global__ void __launch_bounds__(256) k_reduce_contig(const __grid_constant__ LoopArgs a, int64_t rchunk) {
+template <class A, bool VEC, class I>
+__global__ void __launch_bounds__(256) k_reduce_contig(const __grid_constant__ LoopArgs a, int64_t rchunk,
+                                                       FastDiv chdiv) {
   using T = typename A::T;
   constexpr int V = VEC ? (16 / sizeof(T) > 0 ? 16 / sizeof(T) : 1) : 1;
-  constexpr int U = 4;
+  constexpr int U = 8;
   __shared__ T sh[32];
   const T sx = scalar_as<T>(a.sx), sy = scalar_as<T>(a.sy);
   const T* x = static_cast<const T*>(a.x[0]);
@@ -236,17 +244,22 @@ __global__ void __launch_bounds__(256) k_reduce_contig(const __grid_constant__ L
     const int64_t yoff = loop_outer_offsets<1>(a, o, off);
     const int64_t rbeg = split * rchunk;
     const int64_t rend = min(R, rbeg + rchunk);
-    const int64_t units = (rend - rbeg) * chunks;
+    // offsets inside one split in I (int32 when the split's span fits)
+    const I units = (I)((rend - rbeg) * chunks);
+    const I ich = (I)chunks, irs = (I)rs;
+    const T* xb = x + off[0] + rbeg * rs;
     T acc = A::zero();
-    for (int64_t u0 = threadIdx.x; u0 < units; u0 += (int64_t)blockDim.x * U) {
+    for (I u0 = threadIdx.x; u0 < units; u0 += (I)blockDim.x * U) {
       T part[U][V];
 #pragma unroll
       for (int j = 0; j < U; ++j) {
-        const int64_t u = u0 + (int64_t)j * blockDim.x;
+        const I u = u0 + (I)j * (I)blockDim.x;
         if (u < units) {
-          const int64_t r = rbeg + u / chunks;
-          const int64_t c = u - (u / chunks) * chunks;
-          const T* p = x + off[0] + r * rs + c * V;
+          I r;
+          if constexpr (sizeof(I) == 4) r = (I)fast_div((uint32_t)u, chdiv);
+          else r = u / ich;
+          const I c = u - r * ich;
+          const T* p = xb + (I)(r * irs) + (I)(c * V);
           if constexpr (VEC) {
             const uint4 w = __ldg(reinterpret_cast<const uint4*>(p));
             memcpy(&part[j][0], &w, sizeof(w));
@@ -277,8 +290,19 @@ __global__ void __launch_bounds__(256) k_reduce_contig(const __grid_constant__ L
 
 template <class A>
 static cudaError_t launch_reduce_contig_t(const LoopArgs& a, bool vec, int64_t rchunk, int grid, cudaStream_t s) {
-  if (vec) k_reduce_contig<A, true><<<grid, 256, 0, s>>>(a, rchunk);
-  else k_reduce_contig<A, false><<<grid, 256, 0, s>>>(a, rchunk);
+  const int64_t R = a.ninner > 1 ? a.ext[a.nout + 1] : 1;
+  const int64_t rs = a.ninner > 1 ? a.str[1][a.nout + 1] : 0;
+  const bool small = rchunk * (rs > 0 ? rs : 1) + a.ext[a.nout] < ((int64_t)1 << 30) &&
+                     R * a.ext[a.nout] < ((int64_t)1 << 30);
+  constexpr int V = 16 / sizeof(typename A::T) > 0 ? 16 / sizeof(typename A::T) : 1;
+  const FastDiv chdiv = make_fastdiv((uint32_t)(small ? a.ext[a.nout] / (vec ? V : 1) : 1));
+  if (vec) {
+    if (small) k_reduce_contig<A, true, int32_t><<<grid, 256, 0, s>>>(a, rchunk, chdiv);
+    else k_reduce_contig<A, true, int64_t><<<grid, 256, 0, s>>>(a, rchunk, chdiv);
+  } else {
+    if (small) k_reduce_contig<A, false, int32_t><<<grid, 256, 0, s>>>(a, rchunk, chdiv);
+    else k_reduce_contig<A, false, int64_t><<<grid, 256, 0, s>>>(a, rchunk, chdiv);
+  }
   count_launch();
   return cudaGetLastError();
 }
@@ -395,6 +419,80 @@ __global__ void __launch_bounds__(256) k_transpose(const __grid_constant__ PermA
   }
 }
 
+// The same tile transpose when the element count and every offset of x and y
+// fit in 31 bits: offsets in int32 and the per-tile decomposition of the tile
+// index into (y-fast tile, x-fast tile, batch digits) by invariant-divisor
+// multiplies instead of 64-bit divides (the decomposition otherwise costs more
+// instructions than the 2048-element tile's loads and stores).
+struct TransArgs {
+  const void* x;
+  void* y;
+  Scalar sx, sy;
+  int sy_zero, sx_one;
+  int nb;                           // batch modes
+  int32_t e0, et, xs0, xst, ys0, yst;
+  uint32_t ntiles;
+  FastDiv t0, tt;
+  FastDiv bdiv[MAXM];
+  int32_t bxs[MAXM], bys[MAXM];
+};
+
+template <class A, int TY>
+__global__ void __launch_bounds__(256) k_transpose32(const __grid_constant__ TransArgs a) {
+  using T = typename A::T;
+  __shared__ T tile[TY][33];
+  const T sx = scalar_as<T>(a.sx), sy = scalar_as<T>(a.sy);
+  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+  const T* x = static_cast<const T*>(a.x);
+  T* y = static_cast<T*>(a.y);
+  for (uint32_t tid = blockIdx.x; tid < a.ntiles; tid += gridDim.x) {
+    uint32_t r = tid;
+    uint32_t q = fast_div(r, a.t0);
+    const int32_t i0 = (int32_t)(r - q * a.t0.d);
+    r = q;
+    q = fast_div(r, a.tt);
+    const int32_t it = (int32_t)(r - q * a.tt.d);
+    r = q;
+    int32_t xb = 0, yb = 0;
+    for (int m = 0; m < a.nb; ++m) {
+      q = fast_div(r, a.bdiv[m]);
+      const int32_t d = (int32_t)(r - q * a.bdiv[m].d);
+      r = q;
+      xb += d * a.bxs[m];
+      yb += d * a.bys[m];
+    }
+    const int32_t p = it * 32 + tx;
+    const bool pin = p < a.et;
+    const T* xp = x + xb + p * a.xst;
+    const int32_t qb = i0 * TY + ty;
+    T v[TY / 8];
+#pragma unroll
+    for (int k = 0; k < TY / 8; ++k) {
+      const int32_t qq = qb + 8 * k;
+      v[k] = (pin && qq < a.e0) ? xp[qq * a.xs0] : A::zero();
+    }
+#pragma unroll
+    for (int k = 0; k < TY / 8; ++k) tile[ty + 8 * k][tx] = v[k];
+    __syncthreads();
+#pragma unroll
+    for (int h = 0; h < TY / 32; ++h) {
+      const int32_t qq = i0 * TY + 32 * h + tx;
+      if (qq < a.e0) {
+        T* yq = y + yb + qq * a.ys0;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+          const int32_t pp = it * 32 + ty + 8 * k;
+          if (pp < a.et) {
+            T* yp = yq + pp * a.yst;
+            *yp = epilogue<A>(tile[32 * h + tx][ty + 8 * k], yp, sx, sy, a.sy_zero, a.sx_one);
+          }
+        }
+      }
+    }
+    __syncthreads();
+  }
+}
+
 // Elementwise copy in y order (x's fastest mode is y's, or x is broadcast).
 template <class A>
 __global__ void __launch_bounds__(256) k_copy(const __grid_constant__ PermArgs a) {
@@ -459,7 +557,30 @@ static cudaError_t launch_perm_t(const PermArgs& a, int num_sms, cudaStream_t s)
     const int64_t tiles = ((a.ext[0] + TY - 1) / TY) * ((a.ext[a.tmode] + 31) / 32) *
                           (a.n / (a.ext[0] * a.ext[a.tmode]));
     const int grid = (int)(tiles < maxgrid ? tiles : maxgrid);
-    k_transpose<A, TY><<<grid, 256, 0, s>>>(a); count_launch();
+    if (a.n < ((int64_t)1 << 31) && tiles < ((int64_t)1 << 31) &&
+        max_offset(a.nd, a.ext, a.xs) < ((int64_t)1 << 31) &&
+        max_offset(a.nd, a.ext, a.ys) < ((int64_t)1 << 31)) {
+      TransArgs t;
+      t.x = a.x; t.y = a.y; t.sx = a.sx; t.sy = a.sy; t.sy_zero = a.sy_zero; t.sx_one = a.sx_one;
+      t.e0 = (int32_t)a.ext[0]; t.et = (int32_t)a.ext[a.tmode];
+      t.xs0 = (int32_t)a.xs[0]; t.xst = (int32_t)a.xs[a.tmode];
+      t.ys0 = (int32_t)a.ys[0]; t.yst = (int32_t)a.ys[a.tmode];
+      t.ntiles = (uint32_t)tiles;
+      t.t0 = make_fastdiv((uint32_t)((a.ext[0] + TY - 1) / TY));
+      t.tt = make_fastdiv((uint32_t)((a.ext[a.tmode] + 31) / 32));
+      t.nb = 0;
+      for (int m = 1; m < a.nd; ++m) {
+        if (m == a.tmode) continue;
+        t.bdiv[t.nb] = make_fastdiv((uint32_t)a.ext[m]);
+        t.bxs[t.nb] = (int32_t)a.xs[m];
+        t.bys[t.nb] = (int32_t)a.ys[m];
+        ++t.nb;
+      }
+      k_transpose32<A, TY><<<grid, 256, 0, s>>>(t);
+    } else {
+      k_transpose<A, TY><<<grid, 256, 0, s>>>(a);
+    }
+    count_launch();
   } else if (a.nd == 1 && a.xs[0] == 1 && a.ys[0] == 1 && sizeof(T) <= 16 && 16 % sizeof(T) == 0 &&
              ((uintptr_t)a.x % 16) == 0 && ((uintptr_t)a.y % 16) == 0) {
     const int64_t nb = (a.n / (16 / sizeof(T)) + 255) / 256;
