@@ -244,6 +244,37 @@ def tn_section(ome, dev, n=180, sc_target=27):
     return out
 
 
+def tn_sharded_section(ome, dev, world, n=180, sc_target=27):
+    """The n=180 network's slices spread over the ranks (contiguous slice
+    ranges, one NCCL all-reduce of the FP64 partial); device time of one whole
+    contraction, max over ranks."""
+    import torch
+    import torch.distributed as dist
+    code, sd, xs = tn_network(ome, n)
+    opt = ome.optimize_code(code, sd, ome.GreedyMethod(nrepeat=10, seed=0))
+    se = ome.slice_code(opt, sd, ome.GreedySlicer(sc_target=sc_target))
+    d = [torch.from_numpy(x).to(dev) for x in xs]
+    sh = ome.ShardedSlices(se, d)
+    r = sh(d)  # warm-up: plan, workspace, NCCL communicator
+    torch.cuda.synchronize()
+    dist.barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    r = sh(d)
+    e1.record()
+    torch.cuda.synchronize()
+    ome.device_status()
+    t = torch.tensor([e0.elapsed_time(e1)], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    s = float(t.item()) / 1e3
+    return {"workload": f"random 3-regular graph n={n} (seeds 7/8), greedy order (seed 0), sliced to "
+                        f"2^{sc_target} elements, BF16x6", "slices": sh.nslices, "ranks": world,
+            "slices_per_rank": (sh.nslices + world - 1) // world, "s": s, "contractions_per_s": 1.0 / s,
+            "value": float(r.double().cpu()),
+            "parallelism": "contiguous slice ranges per rank, one NCCL all-reduce of the FP64 partial"}
+
+
 def mps_jobs(njobs, seed):
     rng = np.random.default_rng(seed)
     jobs = []
@@ -376,6 +407,8 @@ def main():
     ap.add_argument("--no-tn", action="store_true", help="skip the tensor-network precision section")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched MPS-transfer section")
     ap.add_argument("--no-serve", action="store_true", help="skip the serving section")
+    ap.add_argument("--tn-sharded", action="store_true",
+                    help="run the slice-sharded network section at N=1 too (a one-rank NCCL group)")
     ap.add_argument("--case", default=None,
                     help="profiling aid: run only this suite contraction (e.g. 'ijk->j') twice and exit")
     args = ap.parse_args()
@@ -393,8 +426,14 @@ def main():
     ome = load_package()
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
-    if world > 1:
+    grouped = world > 1 or args.tn_sharded
+    if grouped:
         import datetime
+        if world == 1:
+            os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+            os.environ.setdefault("MASTER_PORT", "29517")
+            os.environ.setdefault("RANK", "0")
+            os.environ.setdefault("WORLD_SIZE", "1")
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     ome.set_einsum_backend(ome.B200Backend(prec=args.prec))
     lib = ome.load_library()
@@ -509,6 +548,7 @@ def main():
     tn = None if (args.no_tn or world > 1) else tn_section(ome, dev)
     ome.release_workspaces()
     torch.cuda.empty_cache()
+    sharded = tn_sharded_section(ome, dev, world) if (grouped and not args.no_tn) else None
     batch = None if (args.no_batch or world > 1) else batch_section(ome, dev)
     serve = None if (args.no_serve or world > 1) else serve_section(ome, dev)
     detail = {}
@@ -529,9 +569,10 @@ def main():
                 "e2e": {"value": e2e_value, "unit": "contractions/s", "h2d_bytes_per_step": h2d,
                         "d2h_bytes_per_step": d2h},
                 "gpu_launches": int(launches), "roofline": roof, "cpu_baseline": cpu,
-                "clocks": cs.summary(), "tn_precision": tn, "batching": batch, "serving": serve}
+                "clocks": cs.summary(), "tn_precision": tn, "tn_sharded": sharded, "batching": batch,
+                "serving": serve}
         print(json.dumps(line), flush=True)
-    if world > 1:
+    if grouped:
         dist.destroy_process_group()
 
 

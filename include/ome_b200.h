@@ -162,6 +162,31 @@ OME_API int ome_plan_execute(ome_ctx* ctx, ome_plan* plan, void* stream,
                      const void* const* inputs, void* y, const void* sx,
                      const void* sy);
 
+/* Slice sharding (the slice loop of src/slicing.jl:118-137 split over ranks;
+ * replaces the host-staged examples/slicing_multigpu.jl:54-75).  The slice
+ * index space 0..nslices-1 is CartesianIndices order over the sliced labels,
+ * first label fastest (src/slicing.jl:37-50).
+ *
+ * ome_plan_slice_count: number of slices (1 for an unsliced plan).
+ * ome_plan_partial_info: the partial a range of slices produces -- dtype
+ *   (F64 for F32/F64 plans with slices, C64 for C32 ones, the plan's dtype
+ *   otherwise), its bytes (the full output, column-major contiguous) and how
+ *   partials of different ranks combine: op 0 = elementwise sum, op 1 =
+ *   elementwise max (Tropical max-plus, Bool or-and).
+ * ome_plan_execute_slices: partial <- (+) over slices [begin, end) of the
+ *   tree value, each at its sliced output positions (the algebra's zero
+ *   elsewhere); sx/sy are not applied.
+ * ome_plan_finish: y <- sy*y + sx*partial, rounded to the plan's dtype.
+ * execute_slices(0, nslices) followed by finish equals ome_plan_execute. */
+OME_API int ome_plan_slice_count(const ome_plan* plan, int64_t* nslices);
+OME_API int ome_plan_partial_info(const ome_plan* plan, int* partial_dtype, size_t* partial_bytes,
+                                  int* reduce_op);
+OME_API int ome_plan_execute_slices(ome_ctx* ctx, ome_plan* plan, void* stream,
+                                    const void* const* inputs, int64_t slice_begin,
+                                    int64_t slice_end, void* partial);
+OME_API int ome_plan_finish(ome_ctx* ctx, ome_plan* plan, void* stream, const void* partial,
+                            void* y, const void* sx, const void* sy);
+
 /* cost_and_gradient (src/bp.jl:122-130): forward with every intermediate kept
  * in the workspace, then einsum_grad (src/autodiff.jl:24-30) per node.
  * dy: the output cotangent (NULL = ones, requires a scalar output).  y

@@ -22,7 +22,8 @@ PREC_AUTO, PREC_FP32, PREC_BF16X3, PREC_BF16X6 = range(4)
 EXPORTS = [
     "ome_version", "ome_launch_count", "ome_device_status", "ome_last_error", "ome_ctx_create", "ome_ctx_destroy", "ome_ctx_workspace_bytes",
     "ome_einsum", "ome_loop_einsum", "ome_plan_create", "ome_plan_destroy", "ome_plan_peak_bytes",
-    "ome_plan_execute", "ome_plan_gradient", "ome_reduce_noalloc", "ome_batch_create", "ome_batch_run",
+    "ome_plan_execute", "ome_plan_gradient", "ome_plan_slice_count", "ome_plan_partial_info",
+    "ome_plan_execute_slices", "ome_plan_finish", "ome_reduce_noalloc", "ome_batch_create", "ome_batch_run",
     "ome_batch_info", "ome_batch_destroy",
 ]
 
@@ -84,6 +85,10 @@ def load() -> C.CDLL:
         lib.ome_plan_peak_bytes.argtypes = [P, C.POINTER(C.c_size_t), C.POINTER(C.c_size_t)]
         lib.ome_plan_execute.argtypes = [P, P, P, C.POINTER(P), P, P, P]
         lib.ome_plan_gradient.argtypes = [P, P, P, C.POINTER(P), P, P, C.POINTER(P)]
+        lib.ome_plan_slice_count.argtypes = [P, i64p]
+        lib.ome_plan_partial_info.argtypes = [P, C.POINTER(C.c_int), C.POINTER(C.c_size_t), C.POINTER(C.c_int)]
+        lib.ome_plan_execute_slices.argtypes = [P, P, P, C.POINTER(P), C.c_int64, C.c_int64, P]
+        lib.ome_plan_finish.argtypes = [P, P, P, P, P, P, P]
         lib.ome_batch_create.argtypes = [P, P, C.c_int, C.c_int32, C.POINTER(Tensor), C.POINTER(Tensor),
                                          C.POINTER(Tensor), C.c_int32, C.POINTER(P)]
         lib.ome_batch_run.argtypes = [P, P, P, P, P]

@@ -453,6 +453,22 @@ static int reduce_dangling(ome_ctx* ctx, cudaStream_t s, ome_dtype dt, HView& xu
   return OME_OK;
 }
 
+// Tensor-core kernel for an FP32 GEMM: 1 = pre-split operands + bulk-copy
+// persistent kernel (k_gemm_packed), 0 = in-kernel converters
+// (k_gemm_bf16x3).  The environment variable OME_GEMM=packed|fused overrides
+// the shape rule.
+static int gemm_kernel_choice(const GemmArgs& g) {
+  static const int forced = [] {
+    const char* e = getenv("OME_GEMM");
+    if (!e) return -1;
+    if (!strcmp(e, "packed")) return 1;
+    if (!strcmp(e, "fused")) return 0;
+    return -1;
+  }();
+  if (forced >= 0) return forced;
+  return 0;
+}
+
 static int run_binary(ome_ctx* ctx, cudaStream_t s, ome_dtype dt, HView x1, HView x2, const HView& yu,
                       const Scalar& sx, const Scalar& sy, bool sy_zero, int prec) {
   OME_CK(reduce_dangling(ctx, s, dt, x1, x2, yu));
@@ -527,6 +543,11 @@ static int run_binary(ome_ctx* ctx, cudaStream_t s, ome_dtype dt, HView x1, HVie
       size_t avail = ctx->ws_bytes > ctx->ws_top ? ctx->ws_bytes - ((ctx->ws_top + 255) & ~(size_t)255) : 0;
       void* w = avail ? ctx->ws + ((ctx->ws_top + 255) & ~(size_t)255) : nullptr;
       const int nterms = prec == OME_PREC_BF16X3 ? 2 : 3;
+      if (gemm_kernel_choice(g) == 1) {
+        cudaError_t e = launch_gemm_packed(g, nterms, w, avail, ctx->num_sms, s);
+        if (e != cudaErrorNotSupported) return cuda_err(e, "packed bf16 split gemm");
+        cudaGetLastError();
+      }
       cudaError_t e = launch_gemm_split(g, nterms, w, avail, ctx->num_sms, s);
       if (e != cudaErrorNotSupported) return cuda_err(e, "bf16 split gemm");
       cudaGetLastError();

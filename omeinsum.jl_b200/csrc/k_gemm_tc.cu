@@ -518,6 +518,455 @@ cudaError_t launch_gemm_split(const GemmArgs& g, int nterms, void* workspace, si
   return cudaGetLastError();
 }
 
+// ===========================================================================
+// Pre-split operands + bulk-copy-fed persistent GEMM
+// ===========================================================================
+//
+// k_pack_split writes each operand once as BF16 terms, already in the UMMA
+// K-major canonical layout: for every (batch, 128-row tile, 32-wide k-step)
+// one contiguous blob of NT 8 KB term tiles.  The GEMM then moves a whole
+// stage with two cp.async.bulk copies (no tensor map, no converter warps):
+//  * warp 8 lane 0 (producer) issues the bulk copies into a STAGES-deep ring,
+//    completion counted by the stage's mbarrier (expect_tx);
+//  * warp 9 allocates TMEM; its lane 0 issues the MMAs exactly as
+//    k_gemm_bf16x3 does (main t0*t0 and cross-term accumulators, two TMEM
+//    buffers, a fresh accumulation every CHUNK k-steps);
+//  * warps 0-7 drain each finished chunk (tcgen05.ld) into FP32 running sums
+//    held in registers (thread = one row x 64 columns), round-to-nearest
+//    adds, and store the tile (αβ epilogue, or a split partial).
+// The kernel is persistent over work units: the first F tiles (whole waves of
+// the grid) are computed whole, the remaining tiles are cut into S K-splits so
+// that the last wave fills the SMs; split partials are summed in split order
+// by k_splitk_tiles (deterministic).  The chunk counter runs across units, so
+// the epilogue of one unit overlaps the MMAs of the next.
+namespace pk {
+constexpr int BM = 128, BN = 128, BK = 32, CHUNK = 8;
+constexpr int TILE_BYTES = BM * BK * 2;     // one term of one operand for one k-step
+constexpr int NDRAIN = 256;                 // drain / epilogue warps 0-7
+constexpr int NTHREADS = NDRAIN + 64;       // + producer warp 8 + MMA warp 9
+constexpr int TMEM_COLS = 512;
+template <int NT> struct Cfg {
+  static constexpr int BLOB = NT * TILE_BYTES;
+  static constexpr int STAGE_BYTES = 2 * BLOB;
+  static constexpr int STAGES = NT == 2 ? 6 : 4;
+  static constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 256;
+};
+}  // namespace pk
+
+struct PackArgs {
+  const float* X;
+  unsigned char* P;   // [L][RT][NKT] blobs of NT x 8 KB
+  int64_t R, K, L, RT, NKT;
+  int nr, nk, nl, kfast;
+  int64_t r_ext[MAXG], r_str[MAXG], k_ext[MAXG], k_str[MAXG], l_ext[MAXG], l_str[MAXG];
+};
+
+struct PkArgs {
+  GemmArgs g;                  // C, M, N, L and the epilogue
+  const unsigned char* PA;     // packed A [L][TM][NKT]
+  const unsigned char* PB;     // packed B [L][TN][NKT]
+  float* partial;              // [(tiles - F) * S][BN][BM]
+  int64_t TM, TN, NKT, tiles, F, ksplit, units;
+  int S;
+};
+
+template <int NT>
+__global__ void __launch_bounds__(256) k_pack_split(const __grid_constant__ PackArgs p) {
+  using namespace pk;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int64_t nblobs = p.L * p.RT * p.NKT;
+  for (int64_t b = blockIdx.x; b < nblobs; b += gridDim.x) {
+    const int64_t kt = b % p.NKT;
+    const int64_t r2 = b / p.NKT;
+    const int64_t rt = r2 % p.RT;
+    const int64_t l = r2 / p.RT;
+    const int64_t loff = mode_offset(l, p.nl, p.l_ext, p.l_str);
+    uint4* out = reinterpret_cast<uint4*>(p.P + b * (int64_t)(NT * TILE_BYTES));
+    float v[2][8];
+    int so[2];
+#pragma unroll
+    for (int j = 0; j < 2; ++j) {
+      // the converter mapping of k_gemm_bf16x3 over 16 virtual warps: each
+      // quarter-warp writes one contiguous 128-byte core matrix
+      const int vw = warp + 8 * j;
+      int row, kc;
+      if (p.kfast) { row = 8 * vw + (lane & 7); kc = lane >> 3; }
+      else { row = 32 * (vw & 3) + lane; kc = vw >> 2; }
+      const int64_t r = rt * BM + row;
+      const int64_t roff = r < p.R ? loff + goff(r, p.nr, p.r_ext, p.r_str) : -1;
+      load_unit(p.X, roff, kt * BK + kc * 8, p.K, p.kfast, p.nk, p.k_ext, p.k_str, v[j]);
+      so[j] = ((row >> 3) * 4 + kc) * 8 + (row & 7);
+    }
+#pragma unroll
+    for (int j = 0; j < 2; ++j) {
+      uint4 t[NT];
+      split8<NT>(v[j], t);
+#pragma unroll
+      for (int u = 0; u < NT; ++u) out[u * (TILE_BYTES / 16) + so[j]] = t[u];
+    }
+  }
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ void bulk_g2s(uint32_t dst, const void* src, uint32_t bytes, uint64_t* bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+               "l"(src), "r"(bytes), "r"(smem_u32(bar))
+               : "memory");
+}
+// Time-bounded wait that ignores the abort flag (used only to let this
+// block's own asynchronous copies and MMAs finish before it exits).
+__device__ __forceinline__ void mbar_wait_quiesce(uint64_t* bar, uint32_t parity) {
+  const uint64_t t0 = gtimer();
+  while (!mbar_try_wait(bar, parity))
+    if (gtimer() - t0 > tc::WAIT_NS) {
+      atomicExch(&g_ome_timeout, 1);
+      return;
+    }
+}
+
+template <int NT>
+__global__ void __launch_bounds__(pk::NTHREADS, 1) k_gemm_packed(const __grid_constant__ PkArgs t) {
+  using namespace pk;
+  constexpr int STAGES = Cfg<NT>::STAGES, STAGE_BYTES = Cfg<NT>::STAGE_BYTES, BLOB = Cfg<NT>::BLOB;
+  extern __shared__ __align__(1024) unsigned char smem[];
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem + STAGES * STAGE_BYTES);
+  uint64_t* empty = full + STAGES;
+  uint64_t* chunk_done = empty + STAGES;   // [2]
+  uint64_t* drained = chunk_done + 2;      // [2]
+  uint64_t* final_bar = drained + 2;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(final_bar + 1);
+  volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
+
+  const GemmArgs& g = t.g;
+  const int tid = threadIdx.x;
+  const int warp = tid >> 5, lane = tid & 31;
+  if (tid == 0) {
+    for (int s = 0; s < STAGES; ++s) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], 1);
+    }
+    for (int b = 0; b < 2; ++b) {
+      mbar_init(&chunk_done[b], 1);
+      mbar_init(&drained[b], NDRAIN);
+    }
+    mbar_init(final_bar, 1);
+    *abort_flag = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 9) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                 "r"(TMEM_COLS)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tmem_slot;
+  auto tmem_main = [&](int b) { return tmem + (uint32_t)(256 * b); };
+  auto tmem_cross = [&](int b) { return tmem + (uint32_t)(256 * b + 128); };
+  const uint32_t sbase = smem_u32(smem);
+
+  // unit u -> tile (l, mt, nt; mt fastest), k-step range, split slot (-1: whole)
+  auto decode = [&](int64_t u, int64_t& l, int64_t& mt, int64_t& nt, int64_t& kb, int64_t& ke, int64_t& slot) {
+    int64_t tile;
+    if (u < t.F) {
+      tile = u; kb = 0; ke = t.NKT; slot = -1;
+    } else {
+      const int64_t v = u - t.F;
+      tile = t.F + v / t.S;
+      kb = (v % t.S) * t.ksplit;
+      ke = min(t.NKT, kb + t.ksplit);
+      slot = v;
+    }
+    mt = tile % t.TM;
+    const int64_t r = tile / t.TM;
+    nt = r % t.TN;
+    l = r / t.TN;
+  };
+
+  if (warp == 8) {
+    // ---------------- producer: two bulk copies per stage ----------------
+    if (lane == 0) {
+      uint32_t it = 0;
+      for (int64_t u = blockIdx.x; u < t.units; u += gridDim.x) {
+        int64_t l, mt, nt, kb, ke, slot;
+        decode(u, l, mt, nt, kb, ke, slot);
+        const unsigned char* pa = t.PA + ((l * t.TM + mt) * t.NKT) * (int64_t)BLOB;
+        const unsigned char* pb = t.PB + ((l * t.TN + nt) * t.NKT) * (int64_t)BLOB;
+        bool ok = true;
+        for (int64_t kt = kb; kt < ke; ++kt, ++it) {
+          const int s = it % STAGES;
+          if (it >= (uint32_t)STAGES && !mbar_wait(&empty[s], ((it / STAGES) - 1) & 1, abort_flag)) {
+            ok = false;
+            break;
+          }
+          mbar_expect_tx(&full[s], 2 * BLOB);
+          bulk_g2s(sbase + s * STAGE_BYTES, pa + kt * BLOB, BLOB, &full[s]);
+          bulk_g2s(sbase + s * STAGE_BYTES + BLOB, pb + kt * BLOB, BLOB, &full[s]);
+        }
+        if (!ok) break;
+      }
+      // the copies of the last STAGES issues must land before the block exits
+      for (uint32_t i = it > (uint32_t)STAGES ? it - STAGES : 0; i < it; ++i)
+        mbar_wait_quiesce(&full[i % STAGES], (i / STAGES) & 1);
+    }
+  } else if (warp == 9) {
+    // ---------------- MMA issue ----------------
+    if (lane == 0) {
+      uint32_t it = 0, gc = 0;
+      bool ok = true;
+      for (int64_t u = blockIdx.x; u < t.units && ok; u += gridDim.x) {
+        int64_t l, mt, nt, kb, ke, slot;
+        decode(u, l, mt, nt, kb, ke, slot);
+        const int nk = (int)(ke - kb);
+        for (int j = 0; j < nk; ++j, ++it) {
+          const uint32_t c = gc + j / CHUNK;
+          const int b = c & 1;
+          const bool first = j % CHUNK == 0;
+          if (first && c >= 2 && !mbar_wait(&drained[b], ((c >> 1) - 1) & 1, abort_flag)) { ok = false; break; }
+          const int s = it % STAGES;
+          if (!mbar_wait(&full[s], (it / STAGES) & 1, abort_flag)) { ok = false; break; }
+          tc_fence_after();
+          const uint32_t sb = sbase + s * STAGE_BYTES;
+#pragma unroll
+          for (int kk = 0; kk < 2; ++kk) {
+            const uint32_t off = kk * 256;
+            uint64_t ad[NT], bd[NT];
+#pragma unroll
+            for (int q = 0; q < NT; ++q) {
+              ad[q] = umma_desc(sb + q * TILE_BYTES + off);
+              bd[q] = umma_desc(sb + BLOB + q * TILE_BYTES + off);
+            }
+            const uint32_t keep = (first && kk == 0) ? 0u : 1u;
+            umma_bf16(tmem_main(b), ad[0], bd[0], keep);
+            bool first_cross = true;
+#pragma unroll
+            for (int d = 1; d < NT; ++d)
+#pragma unroll
+              for (int i = 0; i <= d; ++i) {
+                umma_bf16(tmem_cross(b), ad[i], bd[d - i], first_cross ? keep : 1u);
+                first_cross = false;
+              }
+          }
+          umma_commit(&empty[s]);
+          if (j % CHUNK == CHUNK - 1 || j == nk - 1) umma_commit(&chunk_done[b]);
+        }
+        gc += (uint32_t)((nk + CHUNK - 1) / CHUNK);
+      }
+      // every MMA this thread issued must finish before TMEM is freed
+      umma_commit(final_bar);
+      mbar_wait_quiesce(final_bar, 0);
+    }
+  } else {
+    // ---------------- drain + epilogue (warps 0-7) ----------------
+    const int q = warp & 3, h = warp >> 2;
+    const int row = 32 * q + lane;
+    const int col0 = 64 * h;
+    const uint32_t lane_off = (uint32_t)(32 * q) << 16;
+    uint32_t gc = 0;
+    const float sx = scalar_as<float>(g.sx), sy = scalar_as<float>(g.sy);
+    float* Cp = static_cast<float*>(g.C);
+    for (int64_t u = blockIdx.x; u < t.units; u += gridDim.x) {
+      int64_t l, mt, nt, kb, ke, slot;
+      decode(u, l, mt, nt, kb, ke, slot);
+      const int nch = (int)((ke - kb + CHUNK - 1) / CHUNK);
+      float sum[64];
+#pragma unroll
+      for (int j = 0; j < 64; ++j) sum[j] = 0.f;
+      bool ok = true;
+      for (int ci = 0; ci < nch; ++ci, ++gc) {
+        const int b = gc & 1;
+        if (!mbar_wait(&chunk_done[b], (gc >> 1) & 1, abort_flag)) { ok = false; break; }
+        tc_fence_after();
+#pragma unroll
+        for (int hh = 0; hh < 4; ++hh) {
+          uint32_t rm[16], rc[16];
+          __syncwarp();
+          tmem_ld16(tmem_main(b) + lane_off + (uint32_t)(col0 + 16 * hh), rm);
+          tmem_ld16(tmem_cross(b) + lane_off + (uint32_t)(col0 + 16 * hh), rc);
+#pragma unroll
+          for (int j = 0; j < 16; ++j) {
+            const float v = __uint_as_float(rm[j]) + __uint_as_float(rc[j]);
+            sum[16 * hh + j] = ci == 0 ? v : sum[16 * hh + j] + v;
+          }
+        }
+        tc_fence_before();
+        mbar_arrive(&drained[b]);
+      }
+      if (!ok) break;
+      if (slot >= 0) {
+        float* pp = t.partial + (slot * BN + col0) * (int64_t)BM + row;
+#pragma unroll
+        for (int j = 0; j < 64; ++j) pp[(int64_t)j * BM] = sum[j];
+      } else {
+        const int64_t m = mt * BM + row;
+        if (m < g.M) {
+          const int64_t base = mode_offset(l, g.nl, g.l_ext, g.l_sc) + goff(m, g.nm, g.m_ext, g.m_sc);
+          const int64_t n0 = nt * BN + col0;
+#pragma unroll
+          for (int j = 0; j < 64; ++j) {
+            const int64_t n = n0 + j;
+            if (n < g.N) {
+              float* cp = Cp + base + goff(n, g.nn, g.n_ext, g.n_sc);
+              float o = g.sx_one ? sum[j] : sx * sum[j];
+              if (!g.sy_zero) o = fmaf(sy, *cp, o);
+              *cp = o;
+            }
+          }
+        }
+      }
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 9) {
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(pk::TMEM_COLS) : "memory");
+  }
+}
+
+// Sum the S split partials of each split tile in split order; αβ epilogue.
+__global__ void __launch_bounds__(256) k_splitk_tiles(const __grid_constant__ PkArgs t) {
+  using namespace pk;
+  const GemmArgs& g = t.g;
+  const float sx = scalar_as<float>(g.sx), sy = scalar_as<float>(g.sy);
+  float* Cp = static_cast<float*>(g.C);
+  const int64_t total = (t.tiles - t.F) * BM * BN;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t mloc = i % BM;
+    const int64_t r = i / BM;
+    const int64_t nloc = r % BN;
+    const int64_t v = r / BN;
+    const int64_t tile = t.F + v;
+    const int64_t mt = tile % t.TM, r2 = tile / t.TM, nt = r2 % t.TN, l = r2 / t.TN;
+    const int64_t m = mt * BM + mloc, n = nt * BN + nloc;
+    if (m >= g.M || n >= g.N) continue;
+    float acc = 0.f;
+    for (int s = 0; s < t.S; ++s) acc += t.partial[((v * t.S + s) * BN + nloc) * BM + mloc];
+    float* cp = Cp + mode_offset(l, g.nl, g.l_ext, g.l_sc) + goff(m, g.nm, g.m_ext, g.m_sc) +
+                goff(n, g.nn, g.n_ext, g.n_sc);
+    float o = g.sx_one ? acc : sx * acc;
+    if (!g.sy_zero) o = fmaf(sy, *cp, o);
+    *cp = o;
+  }
+}
+
+static void pack_args(PackArgs& p, const float* X, unsigned char* P, int64_t R, int nr, const int64_t* r_ext,
+                      const int64_t* r_str, const GemmArgs& g, const int64_t* k_str, const int64_t* l_str) {
+  memset(&p, 0, sizeof(p));
+  p.X = X;
+  p.P = P;
+  p.R = R;
+  p.K = g.K;
+  p.L = g.L;
+  p.RT = (R + pk::BM - 1) / pk::BM;
+  p.NKT = (g.K + pk::BK - 1) / pk::BK;
+  p.nr = nr;
+  p.nk = g.nk;
+  p.nl = g.nl;
+  for (int i = 0; i < nr; ++i) { p.r_ext[i] = r_ext[i]; p.r_str[i] = r_str[i]; }
+  for (int i = 0; i < g.nk; ++i) { p.k_ext[i] = g.k_ext[i]; p.k_str[i] = k_str[i]; }
+  for (int i = 0; i < g.nl; ++i) { p.l_ext[i] = g.l_ext[i]; p.l_str[i] = l_str[i]; }
+  p.kfast = k_str[0] == 1 && g.k_ext[0] % 8 == 0;
+}
+
+size_t gemm_packed_bytes(const GemmArgs& g, int nterms, int num_sms) {
+  using namespace pk;
+  const int64_t TM = (g.M + BM - 1) / BM, TN = (g.N + BN - 1) / BN, NKT = (g.K + BK - 1) / BK;
+  const size_t blob = (size_t)nterms * TILE_BYTES;
+  // packed operands + at most one grid's worth of split partials
+  return (size_t)g.L * (TM + TN) * NKT * blob + (size_t)num_sms * BM * BN * 4 + 1024;
+}
+
+cudaError_t launch_gemm_packed(const GemmArgs& g, int nterms, void* workspace, size_t ws_bytes, int num_sms,
+                               cudaStream_t s) {
+  using namespace pk;
+  if (!gemm_split_supported(g) || (nterms != 2 && nterms != 3)) return cudaErrorNotSupported;
+  static bool attr_set[2] = {false, false};
+  if (!attr_set[nterms - 2]) {
+    cudaError_t e = nterms == 2 ? cudaFuncSetAttribute(k_gemm_packed<2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                       Cfg<2>::SMEM_BYTES)
+                                : cudaFuncSetAttribute(k_gemm_packed<3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                       Cfg<3>::SMEM_BYTES);
+    if (e != cudaSuccess) return e;
+    attr_set[nterms - 2] = true;
+  }
+  const int64_t TM = (g.M + BM - 1) / BM, TN = (g.N + BN - 1) / BN, NKT = (g.K + BK - 1) / BK;
+  const size_t blob = (size_t)nterms * TILE_BYTES;
+  const size_t bytes_a = (size_t)g.L * TM * NKT * blob, bytes_b = (size_t)g.L * TN * NKT * blob;
+  const int64_t tiles = g.L * TM * TN;
+  const int64_t G = num_sms;
+  // whole tiles for every complete wave; the rest split along K so that the
+  // last wave covers the grid (at least 8 k-steps per split)
+  int64_t F = tiles >= G ? (tiles / G) * G : 0;
+  int64_t Rt = tiles - F;
+  int64_t S = 1;
+  if (Rt > 0) {
+    S = std::max<int64_t>(1, G / Rt);
+    S = std::min<int64_t>(S, std::max<int64_t>(1, NKT / 8));
+  }
+  const int64_t ksplit = (NKT + S - 1) / S;
+  S = (NKT + ksplit - 1) / ksplit;
+  if (S == 1) {
+    F = tiles;
+    Rt = 0;
+  }
+  const size_t bytes_p = (size_t)Rt * S * BM * BN * 4;
+  if (bytes_a + bytes_b + bytes_p + 768 > ws_bytes) return cudaErrorNotSupported;
+  unsigned char* w = static_cast<unsigned char*>(workspace);
+  unsigned char* PA = w;
+  unsigned char* PB = w + ((bytes_a + 255) & ~(size_t)255);
+  float* part = reinterpret_cast<float*>(PB + ((bytes_b + 255) & ~(size_t)255));
+
+  PackArgs pa, pb;
+  pack_args(pa, static_cast<const float*>(g.A), PA, g.M, g.nm, g.m_ext, g.m_sa, g, g.k_sa, g.l_sa);
+  pack_args(pb, static_cast<const float*>(g.B), PB, g.N, g.nn, g.n_ext, g.n_sb, g, g.k_sb, g.l_sb);
+  const int64_t grid_cap = (int64_t)num_sms * 8;
+  const unsigned ga = (unsigned)std::min<int64_t>(g.L * TM * NKT, grid_cap);
+  const unsigned gb = (unsigned)std::min<int64_t>(g.L * TN * NKT, grid_cap);
+  if (nterms == 2) {
+    k_pack_split<2><<<ga, 256, 0, s>>>(pa);
+    k_pack_split<2><<<gb, 256, 0, s>>>(pb);
+  } else {
+    k_pack_split<3><<<ga, 256, 0, s>>>(pa);
+    k_pack_split<3><<<gb, 256, 0, s>>>(pb);
+  }
+  count_launch(2);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+
+  PkArgs t;
+  memset(&t, 0, sizeof(t));
+  t.g = g;
+  t.PA = PA;
+  t.PB = PB;
+  t.partial = part;
+  t.TM = TM;
+  t.TN = TN;
+  t.NKT = NKT;
+  t.tiles = tiles;
+  t.F = F;
+  t.S = (int)S;
+  t.ksplit = ksplit;
+  t.units = F + Rt * S;
+  const unsigned grid = (unsigned)std::min<int64_t>(t.units, G);
+  if (nterms == 2) k_gemm_packed<2><<<grid, NTHREADS, Cfg<2>::SMEM_BYTES, s>>>(t);
+  else k_gemm_packed<3><<<grid, NTHREADS, Cfg<3>::SMEM_BYTES, s>>>(t);
+  count_launch();
+  e = cudaGetLastError();
+  if (e != cudaSuccess || Rt == 0) return e;
+  const int64_t total = Rt * BM * BN;
+  const int64_t nb = (total + 255) / 256;
+  k_splitk_tiles<<<(unsigned)std::min<int64_t>(nb, (int64_t)num_sms * 16), 256, 0, s>>>(t);
+  count_launch();
+  return cudaGetLastError();
+}
+
 int device_status(cudaStream_t s) {
   cudaError_t e = cudaStreamSynchronize(s);
   if (e != cudaSuccess) return -(int)e;

@@ -55,6 +55,11 @@ cudaError_t launch_fill_one(ome_dtype dt, void* x, int64_t n, cudaStream_t s);
 cudaError_t launch_gemm_split(const GemmArgs& g, int nterms, void* workspace, size_t ws_bytes, int num_sms,
                               cudaStream_t s);
 bool gemm_split_supported(const GemmArgs& g);
+// Pre-split (packed BF16 terms) + bulk-copy-fed persistent GEMM; needs
+// gemm_packed_bytes() of workspace, returns cudaErrorNotSupported otherwise.
+cudaError_t launch_gemm_packed(const GemmArgs& g, int nterms, void* workspace, size_t ws_bytes, int num_sms,
+                               cudaStream_t s);
+size_t gemm_packed_bytes(const GemmArgs& g, int nterms, int num_sms);
 
 // Synchronise s and read/clear the device timeout flag: 1 if a bounded wait
 // gave up, 0 if not, -cudaError on failure.

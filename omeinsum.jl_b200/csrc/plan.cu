@@ -369,6 +369,54 @@ int run_node(ome_ctx* ctx, ome_plan* p, cudaStream_t s, int j, const void* const
 size_t off_fwd_of(const PNode& n) { return n.off_fwd; }
 size_t off_keep_of(const PNode& n) { return n.off_keep; }
 
+
+// Slices [b, e) of the tree, each root result added at its sliced output
+// positions: into the F64/C64 buffer `acc` for acc64 plans (the root goes to
+// the temporary first), else straight into the plan-dtype output `acc` with
+// root scale sx and sy = one (the caller initialised or prescaled it).
+int run_slices(ome_ctx* ctx, ome_plan* p, cudaStream_t s, const void* const* inputs, int64_t b, int64_t e,
+               char* acc, const Scalar& sx) {
+  const ome_dtype dt = p->dt;
+  const Scalar one = scalar_one(dt), zero = scalar_zero(dt);
+  const int root = (int)p->nodes.size() - 1;
+  const PNode& rn = p->nodes[root];
+  const size_t scratch = (p->arena_bytes + 255) & ~(size_t)255;
+  static const std::vector<int32_t> none;
+  static const std::vector<int64_t> nofix;
+  std::vector<int64_t> fix(p->sliced.size(), 0);
+  for (int64_t sl = b; sl < e; ++sl) {
+    int64_t r = sl;
+    for (size_t i = 0; i < p->sliced.size(); ++i) {
+      const int64_t ext = p->ext[p->sliced[i]];
+      fix[i] = r % ext;
+      r /= ext;
+    }
+    for (int j = 0; j < root; ++j) {
+      HView v = make_view(p, ctx->ws + p->nodes[j].off_fwd, p->nodes[j].iy_s, none, nofix);
+      int rc = run_node(ctx, p, s, j, inputs, true, fix, off_fwd_of, v, one, zero, scratch);
+      if (rc) return rc;
+    }
+    if (p->acc64) {
+      HView tv = make_view(p, ctx->ws + p->tmp_off, rn.iy_s, none, nofix);
+      int rc = run_node(ctx, p, s, root, inputs, true, fix, off_fwd_of, tv, one, zero, scratch);
+      if (rc) return rc;
+      // acc[slice positions] += temp
+      const size_t w = dt == OME_C32 ? 16 : 8;
+      HView av = make_view(p, acc, rn.iy, p->sliced, fix);
+      // the accumulator view has element size w: rescale its base offset
+      const int64_t eoff = (av.data - acc) / (int64_t)p->esize;
+      char* abase = acc + eoff * (int64_t)w;
+      rc = cuda_err(launch_acc64_strided(dt, abase, tv.data, av.nd, av.ext, av.str, s), "acc64");
+      if (rc) return rc;
+    } else {
+      HView yv = make_view(p, acc, rn.iy, p->sliced, fix);
+      int rc = run_node(ctx, p, s, root, inputs, true, fix, off_fwd_of, yv, sx, one, scratch);
+      if (rc) return rc;
+    }
+  }
+  return OME_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -411,42 +459,75 @@ int ome_plan_execute(ome_ctx* ctx, ome_plan* p, void* stream, const void* const*
       if (rc) return rc;
     }
   }
-  std::vector<int64_t> fix(p->sliced.size(), 0);
-  for (int64_t sl = 0; sl < p->nslices; ++sl) {
-    int64_t r = sl;
-    for (size_t i = 0; i < p->sliced.size(); ++i) {
-      const int64_t e = p->ext[p->sliced[i]];
-      fix[i] = r % e;
-      r /= e;
-    }
-    for (int j = 0; j < root; ++j) {
-      HView v = make_view(p, ctx->ws + p->nodes[j].off_fwd, p->nodes[j].iy_s, none, nofix);
-      int rc = run_node(ctx, p, s, j, inputs, true, fix, off_fwd_of, v, one, zero, scratch);
-      if (rc) return rc;
-    }
-    if (p->acc64) {
-      HView tv = make_view(p, ctx->ws + p->tmp_off, rn.iy_s, none, nofix);
-      int rc = run_node(ctx, p, s, root, inputs, true, fix, off_fwd_of, tv, one, zero, scratch);
-      if (rc) return rc;
-      // acc[slice positions] += temp
-      const size_t w = dt == OME_C32 ? 16 : 8;
-      HView av = make_view(p, ctx->ws + p->acc_off, rn.iy, p->sliced, fix);
-      // the accumulator view has element size w: rescale its base offset
-      const int64_t eoff = (av.data - (ctx->ws + p->acc_off)) / (int64_t)p->esize;
-      char* abase = ctx->ws + p->acc_off + eoff * (int64_t)w;
-      rc = cuda_err(launch_acc64_strided(dt, abase, tv.data, av.nd, av.ext, av.str, s), "acc64");
-      if (rc) return rc;
-    } else {
-      HView yv = make_view(p, (char*)y, rn.iy, p->sliced, fix);
-      int rc = run_node(ctx, p, s, root, inputs, true, fix, off_fwd_of, yv, sx, one, scratch);
-      if (rc) return rc;
-    }
-  }
+  int rc = run_slices(ctx, p, s, inputs, 0, p->nslices, p->acc64 ? ctx->ws + p->acc_off : (char*)y, sx);
+  if (rc) return rc;
   if (p->acc64) {
     return cuda_err(launch_acc64_store(dt, y, ctx->ws + p->acc_off, rn.numel, sx, sy, scalar_is_zero(dt, sy), s),
                     "acc64 store");
   }
   return OME_OK;
+}
+
+int ome_plan_slice_count(const ome_plan* p, int64_t* nslices) {
+  if (!p || !nslices) return set_err(OME_INVALID_ARGUMENT, "NULL argument");
+  *nslices = p->nslices;
+  return OME_OK;
+}
+
+int ome_plan_partial_info(const ome_plan* p, int* partial_dtype, size_t* partial_bytes, int* reduce_op) {
+  if (!p) return set_err(OME_INVALID_ARGUMENT, "plan is NULL");
+  const int root = (int)p->nodes.size() - 1;
+  const int64_t n = p->nodes[root].numel;
+  ome_dtype pd = p->dt;
+  if (p->acc64) pd = p->dt == OME_C32 ? OME_C64 : OME_F64;
+  if (partial_dtype) *partial_dtype = (int)pd;
+  if (partial_bytes) *partial_bytes = (size_t)n * dtype_size(pd);
+  if (reduce_op) *reduce_op = (p->dt == OME_BOOL || p->dt == OME_TROP_F32 || p->dt == OME_TROP_F64) ? 1 : 0;
+  return OME_OK;
+}
+
+int ome_plan_execute_slices(ome_ctx* ctx, ome_plan* p, void* stream, const void* const* inputs,
+                            int64_t slice_begin, int64_t slice_end, void* partial) {
+  if (!ctx || !p || !inputs || !partial) return set_err(OME_INVALID_ARGUMENT, "NULL argument");
+  if (slice_begin < 0 || slice_end < slice_begin || slice_end > p->nslices)
+    return set_err(OME_INVALID_ARGUMENT, "slice range [%lld, %lld) outside [0, %lld)", (long long)slice_begin,
+                   (long long)slice_end, (long long)p->nslices);
+  if (ctx->ws_bytes < p->fwd_bytes)
+    return set_err(OME_OUT_OF_MEMORY, "plan needs %zu workspace bytes, context has %zu", p->fwd_bytes, ctx->ws_bytes);
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  const int root = (int)p->nodes.size() - 1;
+  const PNode& rn = p->nodes[root];
+  if (p->acc64) {
+    const size_t w = p->dt == OME_C32 ? 16 : 8;
+    int rc = cuda_err(cudaMemsetAsync(partial, 0, (size_t)rn.numel * w, s), "memset");
+    if (rc) return rc;
+  } else {
+    static const std::vector<int32_t> none;
+    static const std::vector<int64_t> nofix;
+    HView pv = make_view(p, (char*)partial, rn.iy, none, nofix);
+    int rc = cuda_err(launch_scale(p->dt, partial, pv.nd, pv.ext, pv.str, scalar_zero(p->dt), 1, ctx->num_sms, s),
+                      "fill");
+    if (rc) return rc;
+  }
+  return run_slices(ctx, p, s, inputs, slice_begin, slice_end, (char*)partial, scalar_one(p->dt));
+}
+
+int ome_plan_finish(ome_ctx* ctx, ome_plan* p, void* stream, const void* partial, void* y, const void* sxp,
+                    const void* syp) {
+  if (!ctx || !p || !partial || !y || !sxp || !syp) return set_err(OME_INVALID_ARGUMENT, "NULL argument");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  const ome_dtype dt = p->dt;
+  const Scalar sx = scalar_from(dt, sxp), sy = scalar_from(dt, syp);
+  const int root = (int)p->nodes.size() - 1;
+  const PNode& rn = p->nodes[root];
+  if (p->acc64)
+    return cuda_err(launch_acc64_store(dt, y, partial, rn.numel, sx, sy, scalar_is_zero(dt, sy), s), "acc64 store");
+  static const std::vector<int32_t> none;
+  static const std::vector<int64_t> nofix;
+  HView xv = make_view(p, (char*)partial, rn.iy, none, nofix);
+  HView yv = make_view(p, (char*)y, rn.iy, none, nofix);
+  ctx->ws_top = 0;
+  return einsum_views(ctx, s, dt, 1, &xv, yv, sx, sy, p->prec, false);
 }
 
 }  // extern "C"

@@ -12,7 +12,9 @@ result copied back.
 """
 from __future__ import annotations
 
+import contextlib
 import ctypes as C
+import threading
 from typing import Any, Dict, List, Sequence, Tuple
 
 import numpy as np
@@ -198,25 +200,71 @@ def _require_b200():
     return be
 
 
+# Call descriptors (ctypes tensor structs) by layout, per host thread: a
+# repeated call with the same codes, shapes, strides and dtype only rewrites
+# the data pointers.
+_TLS = threading.local()
+_CALLS_MAX = 4096
+_SCALARS: Dict[Any, C.Array] = {}
+
+
+def _scalar_cached(ome: int, v) -> C.Array:
+    try:
+        key = (ome, type(v), v)
+        b = _SCALARS.get(key)
+    except TypeError:  # unhashable scalar (e.g. a 0-d array)
+        return _scalar_buf(ome, v)
+    if b is None:
+        b = _scalar_buf(ome, v)
+        if len(_SCALARS) < 1024:
+            _SCALARS[key] = b
+    return b
+
+
 def _run_eincode(ixs, iy, p: _Prepared, y: torch.Tensor, sx, sy, loop_only=False, prec=None):
     be = _require_b200()
-    lm = _LabelMap()
-    keep: list = []
-    xs = (_lib.Tensor * len(ixs))()
-    for i, (ix, t) in enumerate(zip(ixs, p.tensors)):
-        if len(ix) != t.dim():
-            raise ArgumentError(f"indices {tuple(ix)} invalid for tensor with ndims = {t.dim()}")
-        xs[i] = _tensor_struct(t, [lm(l) for l in ix], keep)
-    yt = _tensor_struct(y, [lm(l) for l in iy], keep)
-    sxb, syb = _scalar_buf(p.ome, sx), _scalar_buf(p.ome, sy)
-    ctx = _lib.context(y.device.index if y.device.index is not None else torch.cuda.current_device())
-    lib = _lib.load()
     prec = be.prec if prec is None else prec
-    with torch.cuda.device(y.device):
+    ts = p.tensors
+    try:
+        key = (tuple(map(tuple, ixs)), tuple(iy), p.ome, loop_only, prec,
+               tuple((tuple(t.shape), t.stride()) for t in ts), tuple(y.shape), y.stride())
+        hash(key)
+    except TypeError:  # unhashable labels
+        key = None
+    calls = getattr(_TLS, "calls", None)
+    if calls is None:
+        calls = _TLS.calls = {}
+    hit = calls.get(key) if key is not None else None
+    if hit is None:
+        lm = _LabelMap()
+        keep: list = []
+        xs = (_lib.Tensor * len(ixs))()
+        for i, (ix, t) in enumerate(zip(ixs, ts)):
+            if len(ix) != t.dim():
+                raise ArgumentError(f"indices {tuple(ix)} invalid for tensor with ndims = {t.dim()}")
+            xs[i] = _tensor_struct(t, [lm(l) for l in ix], keep)
+        yt = _tensor_struct(y, [lm(l) for l in iy], keep)
+        hit = (xs, yt, keep)
+        if key is not None:
+            if len(calls) >= _CALLS_MAX:
+                calls.pop(next(iter(calls)))
+            calls[key] = hit
+    else:
+        xs, yt, _ = hit
+        for i, t in enumerate(ts):
+            xs[i].data = t.data_ptr()
+        yt.data = y.data_ptr()
+    sxb, syb = _scalar_cached(p.ome, sx), _scalar_cached(p.ome, sy)
+    dev = y.device.index if y.device.index is not None else torch.cuda.current_device()
+    ctx = _lib.context(dev)
+    lib = _lib.load()
+    same = dev == torch.cuda.current_device()
+    with contextlib.nullcontext() if same else torch.cuda.device(dev):
+        st = C.c_void_p(torch.cuda.current_stream().cuda_stream)
         if loop_only:
-            rc = lib.ome_loop_einsum(ctx.handle, _stream(y.device), p.ome, len(ixs), xs, C.byref(yt), sxb, syb)
+            rc = lib.ome_loop_einsum(ctx.handle, st, p.ome, len(ixs), xs, C.byref(yt), sxb, syb)
         else:
-            rc = lib.ome_einsum(ctx.handle, _stream(y.device), p.ome, len(ixs), xs, C.byref(yt), sxb, syb, prec)
+            rc = lib.ome_einsum(ctx.handle, st, p.ome, len(ixs), xs, C.byref(yt), sxb, syb, prec)
     check(rc)
     return y
 

@@ -936,6 +936,33 @@ def sliced_einsum(slicing, ne, xs, size_dict, alg=None, acc_dtype=None):
     return res
 
 
+def sliced_partial(slicing, ne, xs, size_dict, begin, end, alg=None, acc_dtype=None):
+    """The body of ``einsum(::SlicedEinsum)`` (``src/slicing.jl:123-137``) over
+    the slices ``begin..end-1`` of the ``SliceIterator`` order only: the
+    algebra's zero everywhere, then every slice's tree value added at its
+    sliced output positions.  Partials of disjoint ranges combine with the
+    algebra's addition (sum; max for max-plus; or for Bool) into the full
+    cross-slice result."""
+    ixsv = getixsv(ne)
+    iyv = list(ne.iy)
+    res = get_output_array(xs, [size_dict[l] for l in iyv], True, alg)
+    if acc_dtype is not None:
+        res = res.astype(acc_dtype)
+    sd = dict(size_dict)
+    for l in slicing:
+        sd[l] = 1
+    eins = drop_slicedim(ne, slicing)
+    a = algebra_for(res, alg)
+    for k, sm in enumerate(slice_iterator(slicing, size_dict)):
+        if k < begin or k >= end:
+            continue
+        xsi = [take_slice(x, ix, sm) for x, ix in zip(xs, ixsv)]
+        resi = nested_einsum(eins, xsi, sd, alg)
+        sl = tuple(sm[l] if l in sm else slice(None) for l in iyv)
+        res[sl] = a.add(res[sl], resi.astype(res.dtype))
+    return res
+
+
 # ----------------------------------------------------------------------------
 # autodiff (src/autodiff.jl:24-33, src/bp.jl:24-160)
 # ----------------------------------------------------------------------------
