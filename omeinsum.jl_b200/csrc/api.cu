@@ -466,7 +466,9 @@ static int gemm_kernel_choice(const GemmArgs& g) {
     return -1;
   }();
   if (forced >= 0) return forced;
-  return 0;
+  // pre-splitting pays for itself on large GEMMs only (two extra HBM passes)
+  const double flops = 2.0 * (double)g.M * (double)g.N * (double)g.K * (double)g.L;
+  return g.M >= 256 && g.N >= 256 && flops >= 1e9 ? 1 : 0;
 }
 
 static int run_binary(ome_ctx* ctx, cudaStream_t s, ome_dtype dt, HView x1, HView x2, const HView& yu,
@@ -539,6 +541,12 @@ static int run_binary(ome_ctx* ctx, cudaStream_t s, ome_dtype dt, HView x1, HVie
     g.sx_one = scalar_is_one(dt, sx);
     trace_path("gemm M=%lld N=%lld K=%lld L=%lld modes=%d/%d/%d/%d afast=%d bfast=%d prec=%d", (long long)M,
                (long long)N, (long long)K, (long long)L, gm.n, gn.n, gk.n, gl.n, g.a_m_fast, g.b_n_fast, prec);
+    // FP32 batches of small GEMMs (M, N <= 64; tensor-core tiles would be mostly
+    // padding with a few k-steps each): plain FP32 on CUDA cores
+    if (dt == OME_F32 && M <= 64 && N <= 64 && L >= 8) {
+      trace_path("  -> simt 64x64");
+      return cuda_err(launch_gemm_simt_small_f32(g, s), "simt small gemm");
+    }
     if (dt == OME_F32 && prec != OME_PREC_FP32 && gemm_split_supported(g)) {
       size_t avail = ctx->ws_bytes > ctx->ws_top ? ctx->ws_bytes - ((ctx->ws_top + 255) & ~(size_t)255) : 0;
       void* w = avail ? ctx->ws + ((ctx->ws_top + 255) & ~(size_t)255) : nullptr;

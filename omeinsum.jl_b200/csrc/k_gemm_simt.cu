@@ -17,16 +17,19 @@ template <> struct SimtCfg<1> { static constexpr int BM = 128, BN = 128, BK = 8,
 template <> struct SimtCfg<4> { static constexpr int BM = 128, BN = 128, BK = 8, TM = 8, TN = 8; };
 template <> struct SimtCfg<8> { static constexpr int BM = 64, BN = 64, BK = 8, TM = 4, TN = 4; };
 template <> struct SimtCfg<16> { static constexpr int BM = 64, BN = 64, BK = 8, TM = 4, TN = 4; };
+// 64 x 64 tiles for 4-byte types when M and N both fit in 64 (batched small
+// GEMMs such as bij,bjk->bik with 64^3 per batch: a 128 x 128 tile would be
+// three-quarters padding).
+struct SimtSmall { static constexpr int BM = 64, BN = 64, BK = 8, TM = 4, TN = 4; };
 
 __device__ __forceinline__ int64_t group_off(int64_t i, int n, const int64_t* ext, const int64_t* str) {
   if (n == 1) return i * str[0];
   return mode_offset(i, n, ext, str);
 }
 
-template <class A>
+template <class A, class C = SimtCfg<sizeof(typename A::T)>>
 __global__ void __launch_bounds__(256) k_gemm_simt(const __grid_constant__ GemmArgs g) {
   using T = typename A::T;
-  using C = SimtCfg<sizeof(T)>;
   constexpr int BM = C::BM, BN = C::BN, BK = C::BK, TM = C::TM, TN = C::TN;
   constexpr int NT = 256;
   constexpr int RA = BM * BK / NT, RB = BN * BK / NT;
@@ -152,6 +155,15 @@ static cudaError_t launch_gemm_simt_t(const GemmArgs& g, cudaStream_t s) {
   const int64_t gl = g.L < 65535 ? g.L : 65535;
   dim3 grid((unsigned)gm, (unsigned)gn, (unsigned)gl);
   k_gemm_simt<A><<<grid, 256, 0, s>>>(g); count_launch();
+  return cudaGetLastError();
+}
+
+cudaError_t launch_gemm_simt_small_f32(const GemmArgs& g, cudaStream_t s) {
+  if (g.M == 0 || g.N == 0 || g.L == 0) return cudaSuccess;
+  if (g.M > SimtSmall::BM || g.N > SimtSmall::BN) return cudaErrorNotSupported;
+  const int64_t gl = g.L < 65535 ? g.L : 65535;
+  k_gemm_simt<AlgF32, SimtSmall><<<dim3(1, 1, (unsigned)gl), 256, 0, s>>>(g);
+  count_launch();
   return cudaGetLastError();
 }
 

@@ -31,6 +31,8 @@ cudaError_t launch_scale(ome_dtype dt, void* y, int nd, const int64_t* ext, cons
 
 // CUDA-core strided batched GEMM over any algebra.
 cudaError_t launch_gemm_simt(ome_dtype dt, const GemmArgs& g, cudaStream_t s);
+// FP32 batched GEMM with M, N <= 64 on CUDA cores (64 x 64 tiles, one per batch).
+cudaError_t launch_gemm_simt_small_f32(const GemmArgs& g, cudaStream_t s);
 
 // acc[i] (double / double2) += (double) src[i] for n elements, contiguous;
 // FP64 cross-slice accumulation.  dt is the element type of src.

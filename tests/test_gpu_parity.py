@@ -182,3 +182,21 @@ def test_empty_extents():
     assert tuple(got.shape) == (2, 0)
     got = ome.ein("ij,jk->ik")(torch.ones(3, 0, device="cuda"), torch.ones(0, 4, device="cuda"))
     assert torch.equal(got.cpu(), torch.zeros(3, 4))
+
+
+@pytest.mark.parametrize("code,sizes", [
+    ("ij,jk->ik", dict(i=512, j=2048, k=512)),            # 16 tiles, every tile split along K
+    ("ij,jk->ik", dict(i=2304, j=256, k=2304)),           # two whole waves of tiles + a remainder wave
+    ("ij,kj->ki", dict(i=1000, j=1536, k=700)),           # ragged tiles, K contiguous in both operands
+    ("bij,bjk->bik", dict(b=4, i=512, j=512, k=512)),     # batched
+    ("abcd,cdef->abef", dict(a=24, b=20, c=16, d=40, e=18, f=30)),
+])
+def test_large_gemm_packed(code, sizes):
+    """GEMMs large enough for the pre-split (packed-operand) tensor-core kernel,
+    FP32 against FP64 at the BF16x6 tolerance."""
+    rng = np.random.default_rng(12)
+    ixs, iy = parse(code)
+    xs = [gen(rng, [sizes[l] for l in ix], "f32") for ix in ixs]
+    got = to_np(ome.einsum(ome.EinCode(ixs, iy), [to_dev(x, "f32") for x in xs], sizes))
+    ome.device_status()
+    assert_match(got, oracle(ixs, iy, xs, sizes, "f32", wide=True), "f32", 1e-6)
