@@ -72,7 +72,9 @@ static void trace_path(const char* fmt, ...) {
   if (!trace_on()) return;
   va_list ap;
   va_start(ap, fmt);
-  vsnprintf(g_trace, sizeof(g_trace), fmt, ap);
+  // a "  -> route" tag is appended to the shape already recorded
+  const size_t at = (fmt[0] == ' ' && fmt[1] == ' ' && fmt[2] == '-') ? strlen(g_trace) : 0;
+  vsnprintf(g_trace + at, sizeof(g_trace) - at, fmt, ap);
   va_end(ap);
 }
 
@@ -466,9 +468,10 @@ static int gemm_kernel_choice(const GemmArgs& g) {
     return -1;
   }();
   if (forced >= 0) return forced;
-  // pre-splitting pays for itself on large GEMMs only (two extra HBM passes)
+  // pre-splitting pays for itself on large GEMMs with a long K only (two
+  // extra HBM passes over the operands; with a short K the output dominates)
   const double flops = 2.0 * (double)g.M * (double)g.N * (double)g.K * (double)g.L;
-  return g.M >= 256 && g.N >= 256 && flops >= 1e9 ? 1 : 0;
+  return g.M >= 256 && g.N >= 256 && g.K >= 512 && flops >= 1e9 ? 1 : 0;
 }
 
 static int run_binary(ome_ctx* ctx, cudaStream_t s, ome_dtype dt, HView x1, HView x2, const HView& yu,
@@ -541,6 +544,12 @@ static int run_binary(ome_ctx* ctx, cudaStream_t s, ome_dtype dt, HView x1, HVie
     g.sx_one = scalar_is_one(dt, sx);
     trace_path("gemm M=%lld N=%lld K=%lld L=%lld modes=%d/%d/%d/%d afast=%d bfast=%d prec=%d", (long long)M,
                (long long)N, (long long)K, (long long)L, gm.n, gn.n, gk.n, gl.n, g.a_m_fast, g.b_n_fast, prec);
+    // batches of small GEMMs with the batch mode innermost in every tensor
+    // (column-major bij,bjk->bik): lanes over consecutive batches
+    if (gemm_bfast_applies(g)) {
+      trace_path("  -> batch-innermost");
+      return cuda_err(launch_gemm_bfast(dt, g, s), "batch-innermost gemm");
+    }
     // FP32 batches of small GEMMs (M, N <= 64; tensor-core tiles would be mostly
     // padding with a few k-steps each): plain FP32 on CUDA cores
     if (dt == OME_F32 && M <= 64 && N <= 64 && L >= 8) {
@@ -548,18 +557,28 @@ static int run_binary(ome_ctx* ctx, cudaStream_t s, ome_dtype dt, HView x1, HVie
       return cuda_err(launch_gemm_simt_small_f32(g, s), "simt small gemm");
     }
     if (dt == OME_F32 && prec != OME_PREC_FP32 && gemm_split_supported(g)) {
+      // output mode groups of several modes: C offset tables for the epilogues
+      if (g.nm > 1 || g.nn > 1) {
+        int64_t* tab = static_cast<int64_t*>(ws_alloc(ctx, (size_t)(M + N) * sizeof(int64_t)));
+        if (tab) OME_CK(cuda_err(launch_c_offsets(g, tab, s), "offset tables"));
+      }
       size_t avail = ctx->ws_bytes > ctx->ws_top ? ctx->ws_bytes - ((ctx->ws_top + 255) & ~(size_t)255) : 0;
       void* w = avail ? ctx->ws + ((ctx->ws_top + 255) & ~(size_t)255) : nullptr;
       const int nterms = prec == OME_PREC_BF16X3 ? 2 : 3;
       if (gemm_kernel_choice(g) == 1) {
         cudaError_t e = launch_gemm_packed(g, nterms, w, avail, ctx->num_sms, s);
-        if (e != cudaErrorNotSupported) return cuda_err(e, "packed bf16 split gemm");
+        if (e != cudaErrorNotSupported) {
+          trace_path("  -> packed");
+          return cuda_err(e, "packed bf16 split gemm");
+        }
         cudaGetLastError();
       }
+      trace_path("  -> tc");
       cudaError_t e = launch_gemm_split(g, nterms, w, avail, ctx->num_sms, s);
       if (e != cudaErrorNotSupported) return cuda_err(e, "bf16 split gemm");
       cudaGetLastError();
     }
+    trace_path("  -> simt");
     return cuda_err(launch_gemm_simt(dt, g, s), "simt gemm");
   }
   HView xs[2] = {x1, x2};

@@ -284,6 +284,11 @@ struct GemmArgs {
   int a_m_fast, b_n_fast;  // 1: the group's first mode is the operand's contiguous one
   Scalar sx, sy;
   int sy_zero, sx_one;
+  // C offsets of every m and every n (device tables, or NULL): filled when a
+  // group has several modes, so that epilogues index a table instead of
+  // evaluating a mixed-radix offset per element
+  const int64_t* m_tab_c;
+  const int64_t* n_tab_c;
 };
 
 // Offset of flat index i over modes (column-major, first mode fastest).

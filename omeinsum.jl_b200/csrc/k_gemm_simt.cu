@@ -158,6 +158,77 @@ static cudaError_t launch_gemm_simt_t(const GemmArgs& g, cudaStream_t s) {
   return cudaGetLastError();
 }
 
+// Batched GEMM whose batch mode is the contiguous one in A, B and C (Julia
+// column-major `bij,bjk->bik`: b fastest) with small M, N: lane = one of 32
+// consecutive batches, so every load and store of a warp is one contiguous
+// 128-byte row; warp w of 8 owns 2 rows of the block's 16 x 8 output tile
+// and keeps 2 x 8 accumulators (small tiles: enough warps in flight to hide
+// the L2 latency of the K loop, which is unrolled by 4); the 8 warps read the
+// same B rows, which the L1 serves after the first.  Plain algebra
+// arithmetic in K order.
+template <class A>
+__global__ void __launch_bounds__(256) k_gemm_bfast(const __grid_constant__ GemmArgs g) {
+  using T = typename A::T;
+  constexpr int TN = 8, RM = 2, WARPS = 8;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int64_t b = (int64_t)blockIdx.x * 32 + lane;
+  if (b >= g.L) return;
+  const int n0 = blockIdx.y * TN;
+  const int m0 = blockIdx.z * (RM * WARPS) + warp * RM;
+  // one mode per group, 32-bit strides inside a batch (checked by the host)
+  const int sma = (int)g.m_sa[0], smc = (int)g.m_sc[0], snb = (int)g.n_sb[0], snc = (int)g.n_sc[0];
+  const int ska = (int)g.k_sa[0], skb = (int)g.k_sb[0];
+  const int M = (int)g.M, N = (int)g.N;
+  const T* ap = static_cast<const T*>(g.A) + mode_offset(b, g.nl, g.l_ext, g.l_sa) + (int64_t)m0 * sma;
+  const T* bp = static_cast<const T*>(g.B) + mode_offset(b, g.nl, g.l_ext, g.l_sb) + (int64_t)n0 * snb;
+  T* cp0 = static_cast<T*>(g.C) + mode_offset(b, g.nl, g.l_ext, g.l_sc) + (int64_t)m0 * smc + (int64_t)n0 * snc;
+  T acc[RM][TN];
+#pragma unroll
+  for (int r = 0; r < RM; ++r)
+#pragma unroll
+    for (int c = 0; c < TN; ++c) acc[r][c] = A::zero();
+#pragma unroll 4
+  for (int64_t k = 0; k < g.K; ++k) {
+    T av[RM], bv[TN];
+#pragma unroll
+    for (int r = 0; r < RM; ++r) av[r] = m0 + r < M ? ap[r * sma] : A::zero();
+#pragma unroll
+    for (int c = 0; c < TN; ++c) bv[c] = n0 + c < N ? bp[c * snb] : A::zero();
+#pragma unroll
+    for (int r = 0; r < RM; ++r)
+#pragma unroll
+      for (int c = 0; c < TN; ++c) acc[r][c] = A::add(acc[r][c], A::mul(av[r], bv[c]));
+    ap += ska;
+    bp += skb;
+  }
+  const T sx = scalar_as<T>(g.sx), sy = scalar_as<T>(g.sy);
+#pragma unroll
+  for (int r = 0; r < RM; ++r)
+#pragma unroll
+    for (int c = 0; c < TN; ++c)
+      if (m0 + r < M && n0 + c < N) {
+        T* cp = cp0 + r * smc + c * snc;
+        *cp = epilogue<A>(acc[r][c], cp, sx, sy, g.sy_zero, g.sx_one);
+      }
+}
+
+bool gemm_bfast_applies(const GemmArgs& g) {
+  auto small = [](int64_t ext, int64_t str) { return ext * (str < 0 ? -str : str) < ((int64_t)1 << 30); };
+  return g.l_sa[0] == 1 && g.l_sb[0] == 1 && g.l_sc[0] == 1 && g.l_ext[0] >= 32 && g.M <= 64 && g.N <= 64 &&
+         g.K <= 1024 && g.L >= 32 && (g.L + 31) / 32 <= 0x7fffffff && g.nm == 1 && g.nn == 1 && g.nk == 1 &&
+         small(g.M, g.m_sa[0]) && small(g.M, g.m_sc[0]) && small(g.N, g.n_sb[0]) && small(g.N, g.n_sc[0]) &&
+         small(g.K, g.k_sa[0]) && small(g.K, g.k_sb[0]);
+}
+
+cudaError_t launch_gemm_bfast(ome_dtype dt, const GemmArgs& g, cudaStream_t s) {
+  if (g.M == 0 || g.N == 0 || g.L == 0) return cudaSuccess;
+  if (!gemm_bfast_applies(g)) return cudaErrorNotSupported;
+  const dim3 grid((unsigned)((g.L + 31) / 32), (unsigned)((g.N + 7) / 8), (unsigned)((g.M + 15) / 16));
+  cudaError_t e = cudaErrorInvalidValue;
+  OME_DISPATCH(dt, ALG, k_gemm_bfast<ALG><<<grid, 256, 0, s>>>(g); count_launch(); e = cudaGetLastError());
+  return e;
+}
+
 cudaError_t launch_gemm_simt_small_f32(const GemmArgs& g, cudaStream_t s) {
   if (g.M == 0 || g.N == 0 || g.L == 0) return cudaSuccess;
   if (g.M > SimtSmall::BM || g.N > SimtSmall::BN) return cudaErrorNotSupported;

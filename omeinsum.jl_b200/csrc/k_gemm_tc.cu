@@ -159,6 +159,14 @@ __device__ __forceinline__ int64_t goff(int64_t i, int n, const int64_t* ext, co
   return mode_offset(i, n, ext, str);
 }
 
+// C offsets of row m / column n (through the tables when present).
+__device__ __forceinline__ int64_t c_moff(const GemmArgs& g, int64_t m) {
+  return g.m_tab_c ? g.m_tab_c[m] : goff(m, g.nm, g.m_ext, g.m_sc);
+}
+__device__ __forceinline__ int64_t c_noff(const GemmArgs& g, int64_t n) {
+  return g.n_tab_c ? g.n_tab_c[n] : goff(n, g.nn, g.n_ext, g.n_sc);
+}
+
 // Split 8 values into NT bf16 terms, x ~ t0 + t1 (+ t2): t0 = bf16_rn(x),
 // t1 = bf16_rn(x - t0), t2 = bf16_rn(x - t0 - t1); 16 B per term.  Packed:
 // one cvt.rn.bf16x2 per pair and term, terms widened back by bit shifts,
@@ -372,7 +380,7 @@ __global__ void __launch_bounds__(tc::NTHREADS, 1) k_gemm_bf16x3(const __grid_co
     const int64_t m = m0 + row;
     if (m < g.M) {
       const int64_t lc = mode_offset(l, g.nl, g.l_ext, g.l_sc);
-      const int64_t cm = goff(m, g.nm, g.m_ext, g.m_sc);
+      const int64_t cm = c_moff(g, m);
       float* Cp = static_cast<float*>(g.C);
       const float sx = scalar_as<float>(g.sx), sy = scalar_as<float>(g.sy);
 #pragma unroll 4
@@ -383,7 +391,7 @@ __global__ void __launch_bounds__(tc::NTHREADS, 1) k_gemm_bf16x3(const __grid_co
         if (t.S > 1) {
           t.partial[((split * g.L + l) * g.N + n) * g.M + m] = v;
         } else {
-          float* cp = Cp + lc + cm + goff(n, g.nn, g.n_ext, g.n_sc);
+          float* cp = Cp + lc + cm + c_noff(g, n);
           float o = g.sx_one ? v : sx * v;
           if (!g.sy_zero) o = fmaf(sy, *cp, o);
           *cp = o;
@@ -450,12 +458,31 @@ __global__ void __launch_bounds__(256) k_splitk_reduce(const __grid_constant__ T
     const int64_t l = r / g.N;
     float acc = 0.f;
     for (int s = 0; s < t.S; ++s) acc += t.partial[((s * g.L + l) * g.N + n) * g.M + m];
-    float* cp = Cp + mode_offset(l, g.nl, g.l_ext, g.l_sc) + goff(m, g.nm, g.m_ext, g.m_sc) +
-                goff(n, g.nn, g.n_ext, g.n_sc);
+    float* cp = Cp + mode_offset(l, g.nl, g.l_ext, g.l_sc) + c_moff(g, m) +
+                c_noff(g, n);
     float o = g.sx_one ? acc : sx * acc;
     if (!g.sy_zero) o = fmaf(sy, *cp, o);
     *cp = o;
   }
+}
+
+// m -> C offset of m and n -> C offset of n for groups of several modes.
+__global__ void __launch_bounds__(256) k_c_offsets(const __grid_constant__ GemmArgs g, int64_t* mt, int64_t* nt) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < g.M + g.N;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    if (i < g.M) mt[i] = mode_offset(i, g.nm, g.m_ext, g.m_sc);
+    else nt[i - g.M] = mode_offset(i - g.M, g.nn, g.n_ext, g.n_sc);
+  }
+}
+
+cudaError_t launch_c_offsets(GemmArgs& g, int64_t* tab, cudaStream_t s) {
+  const int64_t n = g.M + g.N;
+  const int64_t nb = (n + 255) / 256;
+  k_c_offsets<<<(unsigned)(nb < 4096 ? nb : 4096), 256, 0, s>>>(g, tab, tab + g.M);
+  count_launch();
+  g.m_tab_c = tab;
+  g.n_tab_c = tab + g.M;
+  return cudaGetLastError();
 }
 
 bool gemm_split_supported(const GemmArgs& g) {
@@ -805,13 +832,13 @@ __global__ void __launch_bounds__(pk::NTHREADS, 1) k_gemm_packed(const __grid_co
       } else {
         const int64_t m = mt * BM + row;
         if (m < g.M) {
-          const int64_t base = mode_offset(l, g.nl, g.l_ext, g.l_sc) + goff(m, g.nm, g.m_ext, g.m_sc);
+          const int64_t base = mode_offset(l, g.nl, g.l_ext, g.l_sc) + c_moff(g, m);
           const int64_t n0 = nt * BN + col0;
 #pragma unroll
           for (int j = 0; j < 64; ++j) {
             const int64_t n = n0 + j;
             if (n < g.N) {
-              float* cp = Cp + base + goff(n, g.nn, g.n_ext, g.n_sc);
+              float* cp = Cp + base + c_noff(g, n);
               float o = g.sx_one ? sum[j] : sx * sum[j];
               if (!g.sy_zero) o = fmaf(sy, *cp, o);
               *cp = o;
@@ -848,8 +875,8 @@ __global__ void __launch_bounds__(256) k_splitk_tiles(const __grid_constant__ Pk
     if (m >= g.M || n >= g.N) continue;
     float acc = 0.f;
     for (int s = 0; s < t.S; ++s) acc += t.partial[((v * t.S + s) * BN + nloc) * BM + mloc];
-    float* cp = Cp + mode_offset(l, g.nl, g.l_ext, g.l_sc) + goff(m, g.nm, g.m_ext, g.m_sc) +
-                goff(n, g.nn, g.n_ext, g.n_sc);
+    float* cp = Cp + mode_offset(l, g.nl, g.l_ext, g.l_sc) + c_moff(g, m) +
+                c_noff(g, n);
     float o = g.sx_one ? acc : sx * acc;
     if (!g.sy_zero) o = fmaf(sy, *cp, o);
     *cp = o;

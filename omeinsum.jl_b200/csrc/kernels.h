@@ -33,6 +33,10 @@ cudaError_t launch_scale(ome_dtype dt, void* y, int nd, const int64_t* ext, cons
 cudaError_t launch_gemm_simt(ome_dtype dt, const GemmArgs& g, cudaStream_t s);
 // FP32 batched GEMM with M, N <= 64 on CUDA cores (64 x 64 tiles, one per batch).
 cudaError_t launch_gemm_simt_small_f32(const GemmArgs& g, cudaStream_t s);
+// Batched GEMM with the batch mode contiguous in A, B and C and M, N <= 64
+// (lanes = consecutive batches); cudaErrorNotSupported if the shape differs.
+bool gemm_bfast_applies(const GemmArgs& g);
+cudaError_t launch_gemm_bfast(ome_dtype dt, const GemmArgs& g, cudaStream_t s);
 
 // acc[i] (double / double2) += (double) src[i] for n elements, contiguous;
 // FP64 cross-slice accumulation.  dt is the element type of src.
@@ -57,6 +61,9 @@ cudaError_t launch_fill_one(ome_dtype dt, void* x, int64_t n, cudaStream_t s);
 cudaError_t launch_gemm_split(const GemmArgs& g, int nterms, void* workspace, size_t ws_bytes, int num_sms,
                               cudaStream_t s);
 bool gemm_split_supported(const GemmArgs& g);
+// Fill tab[0..M) and tab[M..M+N) with the C offsets of m and n and point
+// g.m_tab_c / g.n_tab_c at them (for mode groups of several modes).
+cudaError_t launch_c_offsets(GemmArgs& g, int64_t* tab, cudaStream_t s);
 // Pre-split (packed BF16 terms) + bulk-copy-fed persistent GEMM; needs
 // gemm_packed_bytes() of workspace, returns cudaErrorNotSupported otherwise.
 cudaError_t launch_gemm_packed(const GemmArgs& g, int nterms, void* workspace, size_t ws_bytes, int num_sms,

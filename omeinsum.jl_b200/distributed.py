@@ -29,7 +29,7 @@ import torch.distributed as dist
 from . import _lib
 from ._lib import ArgumentError, check
 from .core import SlicedEinsum, get_size_dict
-from .engine import TropicalTensor, _alloc, _f_contig, _Prepared, _require_b200, _scalar_buf, _stream
+from .engine import TropicalTensor, _alloc, _f_contig, _Prepared, _require_b200, _scalar_buf, _stream, _to_host
 from .plan import _ptrs, get_plan
 
 SUM, MAX = 0, 1
@@ -154,7 +154,7 @@ class ShardedSlices:
         if y is not None:
             return y
         if self.host:
-            yt = yt.cpu()
+            yt = _to_host(yt)
         return TropicalTensor(yt) if self.ome in (_lib.TROP_F32, _lib.TROP_F64) else yt
 
 

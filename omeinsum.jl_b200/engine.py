@@ -108,6 +108,17 @@ def _f_contig(x: torch.Tensor) -> torch.Tensor:
     return y
 
 
+def _to_host(y: torch.Tensor) -> torch.Tensor:
+    """Device result -> host tensor for callers that passed host inputs: the
+    copy lands in page-locked memory (torch's caching host allocator, reused
+    across calls), which moves at link speed; a pageable copy runs several
+    times slower.  Returns once the data is on the host."""
+    out = torch.empty_strided(tuple(y.shape), tuple(y.stride()), dtype=y.dtype, pin_memory=True)
+    out.copy_(y, non_blocking=True)
+    torch.cuda.current_stream(y.device).synchronize()
+    return out
+
+
 class _Prepared:
     """Inputs moved to one CUDA device with one element type."""
 
@@ -141,7 +152,7 @@ class _Prepared:
 
     def wrap(self, y: torch.Tensor):
         if self.host:
-            y = y.cpu()
+            y = _to_host(y)
         return TropicalTensor(y) if self.tropical else y
 
 
@@ -186,6 +197,22 @@ def _tensor_struct(t: torch.Tensor, labels: Sequence[int], keep: list) -> _lib.T
     labs = (C.c_int32 * max(nd, 1))(*labels)
     keep.extend([dims, strides, labs])
     return _lib.Tensor(t.data_ptr(), nd, dims, strides, labs)
+
+
+# torch's raw queries (what torch.cuda.current_stream / current_device wrap;
+# the wrappers cost several microseconds per call)
+_RAW_STREAM = getattr(torch._C, "_cuda_getCurrentRawStream", None)
+_GET_DEVICE = getattr(torch._C, "_cuda_getDevice", None)
+
+
+def _raw_stream(index: int) -> int:
+    if _RAW_STREAM is not None:
+        return _RAW_STREAM(index)
+    return torch.cuda.current_stream(index).cuda_stream
+
+
+def _current_device() -> int:
+    return _GET_DEVICE() if _GET_DEVICE is not None else torch.cuda.current_device()
 
 
 def _stream(device) -> C.c_void_p:
@@ -255,12 +282,12 @@ def _run_eincode(ixs, iy, p: _Prepared, y: torch.Tensor, sx, sy, loop_only=False
             xs[i].data = t.data_ptr()
         yt.data = y.data_ptr()
     sxb, syb = _scalar_cached(p.ome, sx), _scalar_cached(p.ome, sy)
-    dev = y.device.index if y.device.index is not None else torch.cuda.current_device()
+    cur = _current_device()
+    dev = y.device.index if y.device.index is not None else cur
     ctx = _lib.context(dev)
     lib = _lib.load()
-    same = dev == torch.cuda.current_device()
-    with contextlib.nullcontext() if same else torch.cuda.device(dev):
-        st = C.c_void_p(torch.cuda.current_stream().cuda_stream)
+    with contextlib.nullcontext() if dev == cur else torch.cuda.device(dev):
+        st = C.c_void_p(_raw_stream(dev))
         if loop_only:
             rc = lib.ome_loop_einsum(ctx.handle, st, p.ome, len(ixs), xs, C.byref(yt), sxb, syb)
         else:

@@ -200,3 +200,26 @@ def test_large_gemm_packed(code, sizes):
     got = to_np(ome.einsum(ome.EinCode(ixs, iy), [to_dev(x, "f32") for x in xs], sizes))
     ome.device_status()
     assert_match(got, oracle(ixs, iy, xs, sizes, "f32", wide=True), "f32", 1e-6)
+
+
+@pytest.mark.parametrize("dt", ["f32", "f64", "c64", "i64", "trop", "bool"])
+@pytest.mark.parametrize("code,sizes", [
+    ("bij,bjk->bik", dict(b=100, i=37, j=50, k=23)),     # ragged batch warp, partial 16x16 tiles
+    ("bij,bkj->bki", dict(b=64, i=64, j=9, k=64)),        # transposed operands, full tiles
+    ("bcij,bcjk->bcik", dict(b=40, c=3, i=5, j=7, k=6)),  # two batch modes, b innermost
+])
+def test_batch_innermost_gemm(code, sizes, dt):
+    """Batches of small GEMMs whose batch mode is contiguous in every tensor
+    (column-major bij,bjk->bik), with y <- 2y + 3f for Int64."""
+    rng = np.random.default_rng(13)
+    ixs, iy = parse(code)
+    xs = [gen(rng, [sizes[l] for l in ix], dt) for ix in ixs]
+    c = ome.EinCode(ixs, iy)
+    got = to_np(ome.einsum(c, [to_dev(x, dt) for x in xs], sizes))
+    ome.device_status()
+    assert_match(got, oracle(ixs, iy, xs, sizes, dt), dt)
+    if dt == "i64":
+        y0 = gen(rng, [sizes[l] for l in iy], dt)
+        yd = to_dev(y0, dt)
+        ome.einsum_(c, [to_dev(x, dt) for x in xs], yd, 3, 2, sizes)
+        assert_match(to_np(yd), 3 * oracle(ixs, iy, xs, sizes, dt) + 2 * y0, dt)
