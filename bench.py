@@ -459,7 +459,7 @@ def main():
 
     def flush_l2(i):
         flush.fill_(i)
-        torch.sum(clean, out=sink)
+        torch.sum(clean, dim=0, out=sink)
 
     ev = [[(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in CASES]
           for _ in range(args.steps)]

@@ -20,6 +20,7 @@ from typing import Any, Dict, List, Sequence, Tuple
 
 import numpy as np
 
+from ._lib import ArgumentError
 from .core import AbstractEinsum, EinCode, NestedEinsum, SlicedEinsum
 
 
@@ -328,33 +329,69 @@ def slice_code(code: NestedEinsum, size_dict: Dict[Any, int], slicer: GreedySlic
 # ----------------------------------------------------------------------------
 
 
+# Contraction-tree JSON in the layout of OMEinsumContractionOrders'
+# writejson/readjson, which OMEinsum re-exports (src/contractionorder.jl:48-51;
+# dependency compat "1.1" in the reference's Project.toml): a top-level object
+# with "label-type" ("Char" for one-character string labels, "Int64" for
+# integers), "inputs" (every leaf's labels), "output", "tree" and, for a
+# SlicedEinsum, "slices".  A tree node is {"isleaf": true, "tensorindex": i}
+# with Julia's 1-based index, or {"isleaf": false, "args": [...], "eins":
+# {"ixs": [...], "iy": [...]}}.  Files written by a Julia installation load
+# here and the other way round.
+
+
+def _label_type(labels) -> str:
+    labels = list(labels)
+    if all(isinstance(l, str) and len(l) == 1 for l in labels):
+        return "Char"
+    if all(isinstance(l, int) and not isinstance(l, bool) for l in labels):
+        return "Int64"
+    raise ArgumentError("JSON trees take one-character string labels or integer labels")
+
+
 def _tree_to_obj(ne: NestedEinsum):
     if ne.isleaf:
-        return {"isleaf": True, "tensorindex": ne.tensorindex}
+        return {"isleaf": True, "tensorindex": ne.tensorindex + 1}
     return {"isleaf": False, "args": [_tree_to_obj(a) for a in ne.args],
             "eins": {"ixs": [list(ix) for ix in ne.eins.ixs], "iy": list(ne.eins.iy)}}
 
 
-def _obj_to_tree(o):
+def _obj_to_tree(o, conv, base):
     if o["isleaf"]:
-        return NestedEinsum(int(o["tensorindex"]))
-    return NestedEinsum([_obj_to_tree(a) for a in o["args"]],
-                        EinCode([tuple(ix) for ix in o["eins"]["ixs"]], tuple(o["eins"]["iy"])))
+        return NestedEinsum(int(o["tensorindex"]) - base)
+    return NestedEinsum([_obj_to_tree(a, conv, base) for a in o["args"]],
+                        EinCode([tuple(conv(l) for l in ix) for ix in o["eins"]["ixs"]],
+                                tuple(conv(l) for l in o["eins"]["iy"])))
 
 
 def writejson(filename: str, code) -> None:
-    """Save a NestedEinsum / SlicedEinsum (this package's JSON schema: a nested
-    object per node with ``isleaf``, ``tensorindex`` or ``args`` + ``eins``)."""
+    """``writejson`` (src/contractionorder.jl:48-50): save a NestedEinsum or
+    SlicedEinsum in OMEinsumContractionOrders' JSON layout."""
+    ne = code.eins if isinstance(code, SlicedEinsum) else code
+    ixs, iy = ne.getixsv(), list(ne.getiyv())
+    labels = [l for ix in ixs for l in ix] + iy + (list(code.slicing) if isinstance(code, SlicedEinsum) else [])
+    obj = {"label-type": _label_type(labels), "inputs": [list(ix) for ix in ixs], "output": iy,
+           "tree": _tree_to_obj(ne)}
     if isinstance(code, SlicedEinsum):
-        obj = {"slices": list(code.slicing), "tree": _tree_to_obj(code.eins)}
-    else:
-        obj = {"slices": None, "tree": _tree_to_obj(code)}
+        obj["slices"] = list(code.slicing)
     with open(filename, "w") as f:
         json.dump(obj, f)
 
 
 def readjson(filename: str):
+    """``readjson`` (src/contractionorder.jl:51): load a tree written by
+    ``writejson`` here or by OMEinsumContractionOrders in Julia."""
     with open(filename) as f:
         obj = json.load(f)
-    t = _obj_to_tree(obj["tree"])
-    return t if obj.get("slices") is None else SlicedEinsum(obj["slices"], t)
+    lt = obj.get("label-type")
+    if lt is None:  # this package's earlier layout: 0-based leaves, labels as stored
+        t = _obj_to_tree(obj["tree"], lambda l: l, 0)
+        return t if obj.get("slices") is None else SlicedEinsum(obj["slices"], t)
+    if lt == "Char":
+        conv = lambda l: str(l)[0]
+    elif lt.startswith("Int") or lt.startswith("UInt"):
+        conv = int
+    else:
+        raise ArgumentError(f"label type {lt} is not supported")
+    t = _obj_to_tree(obj["tree"], conv, 1)
+    return t if "slices" not in obj else SlicedEinsum([conv(l) for l in obj["slices"]], t)

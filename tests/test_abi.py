@@ -108,3 +108,41 @@ def test_greedy_bounds_kat():
     assert math.isclose(tc, math.log2(ome.flop(opt, sd)))
     assert 16 <= tc <= math.log2(2 ** 10 + 2 ** 16 + 2 ** 15 + 2 ** 9 + 1e-8)
     assert sc == 11
+
+
+def test_json_layout_interchange(tmp_path):
+    """writejson/readjson use OMEinsumContractionOrders' layout (1-based leaf
+    indices, "label-type", "inputs", "output", "tree", "slices"), so trees
+    written by a Julia installation load here and the other way round."""
+    import json
+    # a tree as OMEinsumContractionOrders writes it for ein"(ij,jk),kl->il" sliced over j
+    julia_file = tmp_path / "julia.json"
+    julia_file.write_text(json.dumps({
+        "label-type": "Char", "inputs": [["i", "j"], ["j", "k"], ["k", "l"]], "output": ["i", "l"],
+        "slices": ["j"],
+        "tree": {"isleaf": False, "eins": {"ixs": [["i", "k"], ["k", "l"]], "iy": ["i", "l"]},
+                 "args": [{"isleaf": False, "eins": {"ixs": [["i", "j"], ["j", "k"]], "iy": ["i", "k"]},
+                           "args": [{"isleaf": True, "tensorindex": 1}, {"isleaf": True, "tensorindex": 2}]},
+                          {"isleaf": True, "tensorindex": 3}]}}))
+    se = ome.readjson(str(julia_file))
+    assert isinstance(se, ome.SlicedEinsum) and list(se.slicing) == ["j"]
+    assert se.eins == ome.ein("(ij,jk),kl->il")
+    # written files carry the same layout: 1-based leaves and the top-level keys
+    out = tmp_path / "out.json"
+    ome.writejson(str(out), se)
+    obj = json.loads(out.read_text())
+    assert obj["label-type"] == "Char" and obj["slices"] == ["j"] and obj["output"] == ["i", "l"]
+    assert obj["inputs"] == [["i", "j"], ["j", "k"], ["k", "l"]]
+    assert obj["tree"]["args"][1] == {"isleaf": True, "tensorindex": 3}
+    assert ome.readjson(str(out)) == se
+    # integer labels
+    code = ome.EinCode([[1, 2], [2, 3], [3, 4]], [1, 4])
+    g = ome.slice_code(ome.optimize_code(code, ome.uniformsize(code, 4), ome.GreedyMethod()),
+                       ome.uniformsize(code, 4), ome.GreedySlicer(sc_target=2))
+    f = tmp_path / "int.json"
+    ome.writejson(str(f), g)
+    assert json.loads(f.read_text())["label-type"] == "Int64"
+    assert ome.readjson(str(f)) == g
+    with pytest.raises(ome.ArgumentError):
+        ome.writejson(str(f), ome.ein("(ab,bc),cd->ad").__class__([ome.NestedEinsum(0), ome.NestedEinsum(1)],
+                                                                    ome.EinCode([("xx", "y"), ("y", "z")], ("xx", "z"))))
