@@ -185,15 +185,16 @@ def test_empty_extents():
 
 
 @pytest.mark.parametrize("code,sizes", [
-    ("ij,jk->ik", dict(i=512, j=2048, k=512)),            # 16 tiles, every tile split along K
-    ("ij,jk->ik", dict(i=2304, j=256, k=2304)),           # two whole waves of tiles + a remainder wave
-    ("ij,kj->ki", dict(i=1000, j=1536, k=700)),           # ragged tiles, K contiguous in both operands
+    ("ij,jk->ik", dict(i=512, j=2048, k=512)),            # 8 tiles of 128x256, every tile split along K
+    ("ij,jk->ik", dict(i=2304, j=512, k=2304)),           # a whole wave of tiles + a split remainder wave
+    ("ij,kj->ki", dict(i=1000, j=1536, k=700)),           # ragged tiles (last 256-wide tile 188 columns)
     ("bij,bjk->bik", dict(b=4, i=512, j=512, k=512)),     # batched
-    ("abcd,cdef->abef", dict(a=24, b=20, c=16, d=40, e=18, f=30)),
+    ("abcd,cdef->abef", dict(a=24, b=20, c=32, d=40, e=18, f=30)),   # multi-mode groups
 ])
 def test_large_gemm_packed(code, sizes):
-    """GEMMs large enough for the pre-split (packed-operand) tensor-core kernel,
-    FP32 against FP64 at the BF16x6 tolerance."""
+    """GEMMs large enough for the pre-split (packed-operand) tensor-core kernel
+    (M, N >= 256, K >= 512, >= 1 GFLOP), FP32 against FP64 at the BF16x6
+    tolerance."""
     rng = np.random.default_rng(12)
     ixs, iy = parse(code)
     xs = [gen(rng, [sizes[l] for l in ix], "f32") for ix in ixs]
