@@ -16,6 +16,7 @@
 //    child's input, the child's labels become the output, result conjugated).
 #include <string.h>
 #include <algorithm>
+#include <cmath>
 #include <map>
 #include <vector>
 
@@ -288,6 +289,44 @@ int ome_plan_create(ome_ctx* ctx, ome_dtype dtype, int32_t ninputs, const int32_
   // per-node dispatch scratch: dangling-label reductions (bounded by the
   // children's sizes), split-reduction partials and GEMM workspace; sliced
   // sizes for the forward plan, full sizes for the (unsliced) gradient
+  // FP32 binary nodes that the dispatcher sends to the packed-operand
+  // tensor-core GEMM (M, N >= 256, K >= 512, >= 1 GFLOP) need their BF16
+  // terms in the workspace: L * (M/128 + N/128 tiles) * K/32 k-steps * 24 KB,
+  // plus split partials and offset tables (at most 2 GB; a node that would
+  // need more runs the in-kernel-converter GEMM instead)
+  auto packed_gemm_bytes = [&](int j, bool use_sliced) -> size_t {
+    const PNode& n = p->nodes[j];
+    if (dtype != OME_F32 || prec == OME_PREC_FP32 || n.args.size() != 2) return 0;
+    auto labs = [&](int r) -> std::vector<int32_t> {
+      std::vector<int32_t> v;
+      if (r >= 0) {
+        v = use_sliced ? p->nodes[r].iy_s : p->nodes[r].iy;
+      } else {
+        for (int32_t l : p->in_labels[-r - 1])
+          if (!(use_sliced && contains(p->sliced, l))) v.push_back(l);
+      }
+      return v;
+    };
+    const std::vector<int32_t> a = labs(n.args[0]), b = labs(n.args[1]);
+    const std::vector<int32_t>& y = use_sliced ? n.iy_s : n.iy;
+    double M = 1, N = 1, K = 1, L = 1;
+    std::vector<int32_t> seen;
+    for (const auto* v : {&a, &b})
+      for (int32_t l : *v) {
+        if (contains(seen, l)) continue;
+        seen.push_back(l);
+        const bool ia = contains(a, l), ib = contains(b, l), iy = contains(y, l);
+        const double e = (double)p->ext[l];
+        if (ia && ib && iy) L *= e;
+        else if (ia && ib) K *= e;
+        else if (ia && iy) M *= e;
+        else if (ib && iy) N *= e;
+      }
+    if (M < 256 || N < 256 || K < 512 || 2.0 * M * N * K * L < 1e9) return 0;
+    const double bytes = L * (std::ceil(M / 128) + std::ceil(N / 128)) * std::ceil(K / 32) * 3 * 8192 +
+                         148.0 * 128 * 128 * 4 + (M + N) * 8 + 4096;
+    return bytes <= (double)((size_t)2 << 30) ? (size_t)bytes : 0;
+  };
   auto scratch_bound = [&](bool use_sliced) {
     size_t scratch = 0;
     for (int j = 0; j < nnodes; ++j) {
@@ -302,6 +341,7 @@ int ome_plan_create(ome_ctx* ctx, ome_dtype dtype, int32_t ninputs, const int32_
         }
         sj += ((size_t)c * p->esize + 255) & ~(size_t)255;
       }
+      sj += packed_gemm_bytes(j, use_sliced);
       scratch = std::max(scratch, sj);
     }
     return scratch + ((size_t)64 << 20);
