@@ -101,6 +101,15 @@ OME_API unsigned long long ome_launch_count(void);
  * result invalid through this flag instead of trapping. */
 OME_API int ome_device_status(void* stream);
 
+/* Failure-path self-test of the bounded device waits (no counterpart in the
+ * reference; the reference's kernels have no device-side waits): launches on
+ * `stream` one block whose thread waits on a shared-memory mbarrier that
+ * nothing arrives on, gives up after `wait_ns` nanoseconds of %globaltimer
+ * (clamped to [1 us, 1 s]), records the timeout flag exactly as a stalled
+ * tensor-core kernel would, and returns.  The next ome_device_status on the
+ * stream reports OME_TIMEOUT once; the context stays usable. */
+OME_API int ome_selftest_wait_timeout(void* stream, uint64_t wait_ns);
+
 /* Message of the last failed call on this host thread ("" if none). */
 OME_API const char* ome_last_error(void);
 
@@ -196,6 +205,27 @@ OME_API int ome_plan_finish(ome_ctx* ctx, ome_plan* plan, void* stream, const vo
 OME_API int ome_plan_gradient(ome_ctx* ctx, ome_plan* plan, void* stream,
                       const void* const* inputs, const void* dy, void* y,
                       void* const* dxs);
+
+/* Contraction-order search (host) ------------------------------------------
+ *
+ * TreeSA: simulated annealing over binary contraction trees, the method
+ * OMEinsum re-exports from OMEinsumContractionOrders (src/contractionorder.jl:
+ * 30-41).  ntensors tensors with nlabels[t] label ids each (concatenated in
+ * `labels`, ids 0..nids-1, log2 extents in log2_sizes), output labels
+ * out_labels.  init_tree / out_tree: ntensors-1 internal nodes in post-order,
+ * two child refs each (r >= 0 internal node, r < 0 input tensor -r-1).
+ * Moves rewrite (A, (B, C)) into ((A, B), C) or ((A, C), B); a move is
+ * accepted with probability min(1, exp(-beta * dcost)), beta from beta_start
+ * to beta_stop in steps of beta_step, niters sweeps over the nodes per beta,
+ * cost = log2(sum 2^tc + rw_weight * 2^rw) + sc_weight * sum max(0, sc -
+ * sc_target) over contractions.  ntrials independent trials (host threads,
+ * seeds derived from `seed`); the best tree is returned with its (tc, sc, rw)
+ * in log2 (out_complexity, 3 doubles; may be NULL). */
+OME_API int ome_treesa(int32_t ntensors, const int32_t* nlabels, const int32_t* labels, int32_t nout,
+                       const int32_t* out_labels, int32_t nids, const double* log2_sizes,
+                       const int32_t* init_tree, double sc_target, double sc_weight, double rw_weight,
+                       double beta_start, double beta_step, double beta_stop, int32_t niters,
+                       int32_t ntrials, uint64_t seed, int32_t* out_tree, double* out_complexity);
 
 /* Batched contractions of uneven shapes (one grouped launch) ----------------
  *

@@ -35,7 +35,8 @@ from .engine import (TropicalTensor, cost_and_gradient, einsum, einsum_, einsum_
 from .batch import BatchedEinsum, capture_graph
 from .serve import Job, TNServer, pow2_rescale
 from .distributed import ShardedSlices, allreduce_partial, sharded_einsum, slice_range
-from .planner import (GreedyMethod, GreedySlicer, contraction_complexity, flop, label_elimination_order,
-                      optimize_code, peak_memory, readjson, slice_code, writejson)
+from .planner import (GreedyMethod, GreedySlicer, MergeVectors, ScoreFunction, TreeSA, TreeSASlicer,
+                      contraction_complexity, flop, label_elimination_order, optimize_code, peak_memory, readjson,
+                      slice_code, writejson)
 
 __all__ = [n for n in dir() if not n.startswith("_")]

@@ -20,11 +20,11 @@ F32, F64, C32, C64, I64, BOOL, TROP_F32, TROP_F64 = range(8)
 PREC_AUTO, PREC_FP32, PREC_BF16X3, PREC_BF16X6 = range(4)
 
 EXPORTS = [
-    "ome_version", "ome_launch_count", "ome_device_status", "ome_last_error", "ome_ctx_create", "ome_ctx_destroy", "ome_ctx_workspace_bytes",
+    "ome_version", "ome_launch_count", "ome_device_status", "ome_selftest_wait_timeout", "ome_last_error", "ome_ctx_create", "ome_ctx_destroy", "ome_ctx_workspace_bytes",
     "ome_einsum", "ome_loop_einsum", "ome_plan_create", "ome_plan_destroy", "ome_plan_peak_bytes",
     "ome_plan_execute", "ome_plan_gradient", "ome_plan_slice_count", "ome_plan_partial_info",
     "ome_plan_execute_slices", "ome_plan_finish", "ome_reduce_noalloc", "ome_batch_create", "ome_batch_run",
-    "ome_batch_info", "ome_batch_destroy",
+    "ome_batch_info", "ome_batch_destroy", "ome_treesa",
 ]
 
 
@@ -74,6 +74,7 @@ def load() -> C.CDLL:
         lib.ome_launch_count.restype = C.c_ulonglong
         lib.ome_last_error.restype = C.c_char_p
         lib.ome_device_status.argtypes = [P]
+        lib.ome_selftest_wait_timeout.argtypes = [P, C.c_uint64]
         lib.ome_ctx_create.argtypes = [C.c_int, C.c_size_t, C.POINTER(P)]
         lib.ome_ctx_destroy.argtypes = [P]
         lib.ome_ctx_workspace_bytes.argtypes = [P, C.POINTER(C.c_size_t)]
@@ -95,6 +96,10 @@ def load() -> C.CDLL:
         lib.ome_batch_info.argtypes = [P, C.POINTER(C.c_int32), C.POINTER(C.c_float)]
         lib.ome_batch_destroy.argtypes = [P]
         lib.ome_reduce_noalloc.argtypes = [P, C.c_int, C.POINTER(Tensor), C.POINTER(Tensor), P, P]
+        dp = C.POINTER(C.c_double)
+        lib.ome_treesa.argtypes = [C.c_int32, i32p, i32p, C.c_int32, i32p, C.c_int32, dp, i32p, C.c_double,
+                                   C.c_double, C.c_double, C.c_double, C.c_double, C.c_double, C.c_int32,
+                                   C.c_int32, C.c_uint64, i32p, dp]
         for f in EXPORTS:
             if f not in ("ome_version", "ome_last_error", "ome_launch_count"):
                 getattr(lib, f).restype = C.c_int

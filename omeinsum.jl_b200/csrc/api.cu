@@ -682,6 +682,10 @@ int ome_device_status(void* stream) {
   return OME_OK;
 }
 
+int ome_selftest_wait_timeout(void* stream, uint64_t wait_ns) {
+  return cuda_err(launch_selftest_wait(wait_ns, static_cast<cudaStream_t>(stream)), "self-test kernel");
+}
+
 const char* ome_last_error(void) { return g_err.c_str(); }
 
 int ome_ctx_create(int device, size_t workspace_bytes, ome_ctx** out) {

@@ -994,6 +994,30 @@ cudaError_t launch_gemm_packed(const GemmArgs& g, int nterms, void* workspace, s
   return cudaGetLastError();
 }
 
+// One thread waits on an mbarrier that nothing arrives on, bounded by
+// wait_ns; on expiry it records the timeout like any stalled wait and exits.
+__global__ void k_selftest_wait(uint64_t wait_ns) {
+  __shared__ __align__(8) uint64_t bar;
+  if (threadIdx.x != 0) return;
+  mbar_init(&bar, 1);
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  const uint64_t t0 = gtimer();
+  while (!mbar_try_wait(&bar, 0)) {
+    if (gtimer() - t0 > wait_ns) {
+      atomicExch(&g_ome_timeout, 1);
+      return;
+    }
+  }
+}
+
+cudaError_t launch_selftest_wait(uint64_t wait_ns, cudaStream_t s) {
+  if (wait_ns < 1000) wait_ns = 1000;
+  if (wait_ns > 1000000000ull) wait_ns = 1000000000ull;
+  k_selftest_wait<<<1, 32, 0, s>>>(wait_ns);
+  count_launch();
+  return cudaGetLastError();
+}
+
 int device_status(cudaStream_t s) {
   cudaError_t e = cudaStreamSynchronize(s);
   if (e != cudaSuccess) return -(int)e;

@@ -73,5 +73,7 @@ size_t gemm_packed_bytes(const GemmArgs& g, int nterms, int num_sms);
 // Synchronise s and read/clear the device timeout flag: 1 if a bounded wait
 // gave up, 0 if not, -cudaError on failure.
 int device_status(cudaStream_t s);
+// One-block kernel whose bounded mbarrier wait runs out (failure-path test).
+cudaError_t launch_selftest_wait(uint64_t wait_ns, cudaStream_t s);
 
 }  // namespace ome

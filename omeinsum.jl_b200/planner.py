@@ -15,7 +15,7 @@ from __future__ import annotations
 
 import json
 import math
-from dataclasses import dataclass
+from dataclasses import dataclass, field
 from typing import Any, Dict, List, Sequence, Tuple
 
 import numpy as np
@@ -40,6 +40,56 @@ class GreedySlicer:
     2^sc_target elements (stand-in for TreeSASlicer(score=ScoreFunction(sc_target)))."""
 
     sc_target: float = 27.0
+
+
+@dataclass
+class ScoreFunction:
+    """Score of a contraction order, OMEinsumContractionOrders' ScoreFunction:
+    time (2^tc) plus rw_weight * read-write (2^rw), with every contraction's
+    space complexity above sc_target penalised by sc_weight per unit of log2."""
+
+    tc_weight: float = 1.0
+    sc_weight: float = 1.0
+    rw_weight: float = 0.0
+    sc_target: float = 20.0
+
+
+@dataclass
+class TreeSA:
+    """Simulated annealing over binary contraction trees (OMEinsumContractionOrders'
+    TreeSA; the search runs natively, ``ome_treesa``).  ``betas`` = (start,
+    step, stop) of the inverse temperature (Julia's 0.01:0.05:15), ``niters``
+    sweeps per temperature, ``ntrials`` independent trials from the
+    ``initializer`` tree ("greedy" or "random")."""
+
+    betas: Tuple[float, float, float] = (0.01, 0.05, 15.0)
+    ntrials: int = 10
+    niters: int = 50
+    initializer: str = "greedy"
+    score: ScoreFunction = field(default_factory=ScoreFunction)
+    seed: int = 0
+
+
+@dataclass
+class TreeSASlicer:
+    """Slicer in the manner of OMEinsumContractionOrders' TreeSASlicer: slice
+    one label at a time (the one that most reduces the space complexity) and
+    re-anneal the tree on the sliced sizes, until the largest intermediate fits
+    2^score.sc_target elements."""
+
+    score: ScoreFunction = field(default_factory=lambda: ScoreFunction(sc_target=20.0))
+    betas: Tuple[float, float, float] = (14.0, 0.05, 15.0)
+    ntrials: int = 2
+    niters: int = 10
+    seed: int = 0
+
+
+@dataclass
+class MergeVectors:
+    """Simplifier: every rank-1 tensor is first multiplied into a tensor that
+    shares its label (OMEinsumContractionOrders' MergeVectors), so the order
+    search sees fewer, larger tensors; the merges become the first nodes of
+    the returned tree."""
 
 
 def _log2sz(labels, log2sd) -> float:
@@ -254,16 +304,156 @@ def label_elimination_order(code: AbstractEinsum) -> List[Any]:
     return order
 
 
-def optimize_code(code: AbstractEinsum, size_dict: Dict[Any, int], optimizer: GreedyMethod | None = None,
-                  slicer: GreedySlicer | None = None):
+def _post_order_pairs(ne: NestedEinsum) -> List[Tuple[int, int]]:
+    """Binary tree -> post-order child-ref pairs (r >= 0 internal, r < 0 leaf -r-1)."""
+    pairs: List[Tuple[int, int]] = []
+
+    def rec(n) -> int:
+        if n.isleaf:
+            return -n.tensorindex - 1
+        if len(n.args) != 2:
+            raise ArgumentError("TreeSA works on binary trees")
+        a, b = rec(n.args[0]), rec(n.args[1])
+        pairs.append((a, b))
+        return len(pairs) - 1
+
+    rec(ne)
+    return pairs
+
+
+def _from_pairs(pairs, ixs, iy) -> NestedEinsum:
+    """Post-order pairs -> NestedEinsum; a node's output labels are the labels
+    of its leaves that occur outside its subtree or in the output."""
+    n = len(ixs)
+    count: Dict[Any, int] = {}
+    for ix in ixs:
+        for l in dict.fromkeys(ix):
+            count[l] = count.get(l, 0) + 1
+    out = set(iy)
+    built: List[Tuple[NestedEinsum, Tuple[Any, ...], Dict[Any, int]]] = []
+
+    def get(r):
+        if r < 0:
+            t = -r - 1
+            c = {}
+            for l in dict.fromkeys(ixs[t]):
+                c[l] = 1
+            return NestedEinsum(t), tuple(ixs[t]), c
+        return built[r]
+
+    for k, (a, b) in enumerate(pairs):
+        na, la, ca = get(a)
+        nb, lb, cb = get(b)
+        c = dict(ca)
+        for l, v in cb.items():
+            c[l] = c.get(l, 0) + v
+        if k == len(pairs) - 1:
+            lab = tuple(iy)
+        else:
+            lab = tuple(l for l in dict.fromkeys(la + lb) if l in out or c[l] < count[l])
+        built.append((NestedEinsum([na, nb], EinCode([la, lb], lab)), lab, c))
+    return built[-1][0]
+
+
+def _merge_vectors(ixs: List[List[Any]]):
+    """MergeVectors: groups (absorbing tensor, vectors merged into it, in order)
+    and the merged network's tensors."""
+    n = len(ixs)
+    absorbed = [False] * n
+    groups: Dict[int, List[int]] = {}
+    for v in range(n):
+        if len(ixs[v]) != 1:
+            continue
+        (l,) = ixs[v]
+        host = next((u for u in range(n) if u != v and not absorbed[u] and len(ixs[u]) > 1 and l in ixs[u]), None)
+        if host is None:
+            continue
+        absorbed[v] = True
+        groups.setdefault(host, []).append(v)
+    keep = [t for t in range(n) if not absorbed[t]]
+    return keep, groups
+
+
+def _expand_merged(ne: NestedEinsum, keep: List[int], groups: Dict[int, List[int]], ixs) -> NestedEinsum:
+    def leaf(t):
+        node = NestedEinsum(t)
+        for v in groups.get(t, []):
+            node = NestedEinsum([node, NestedEinsum(v)], EinCode([tuple(ixs[t]), tuple(ixs[v])], tuple(ixs[t])))
+        return node
+
+    def rec(x):
+        if x.isleaf:
+            return leaf(keep[x.tensorindex])
+        return NestedEinsum([rec(a) for a in x.args], x.eins)
+
+    return rec(ne)
+
+
+def _treesa(ixs: List[List[Any]], iy: List[Any], size_dict, opt: TreeSA, init: NestedEinsum | None = None):
+    """Run ome_treesa on the network and return the best tree as a NestedEinsum."""
+    import ctypes as C
+
+    from . import _lib
+    labels = list(dict.fromkeys([l for ix in ixs for l in ix] + list(iy)))
+    lid = {l: i for i, l in enumerate(labels)}
+    n = len(ixs)
+    if init is None:
+        if opt.initializer == "random":
+            rng = np.random.default_rng(opt.seed)
+            slots = [-(t + 1) for t in range(n)]
+            pairs = []
+            while len(slots) > 1:
+                i, j = rng.choice(len(slots), 2, replace=False)
+                a, b = slots[i], slots[j]
+                pairs.append((a, b))
+                slots = [x for k, x in enumerate(slots) if k not in (i, j)] + [len(pairs) - 1]
+        else:
+            g = optimize_code(EinCode([tuple(ix) for ix in ixs], tuple(iy)), size_dict,
+                              GreedyMethod(nrepeat=1, seed=opt.seed))
+            pairs = _post_order_pairs(g)
+    else:
+        pairs = _post_order_pairs(init)
+    arr = lambda T, v: (T * max(len(v), 1))(*v)
+    nl = [len(ix) for ix in ixs]
+    fl = [lid[l] for ix in ixs for l in ix]
+    ol = [lid[l] for l in iy if l in lid]
+    l2 = [math.log2(max(size_dict[l], 1)) for l in labels]
+    init_arr = [x for p in pairs for x in p]
+    out = (C.c_int32 * (2 * (n - 1)))()
+    cx = (C.c_double * 3)()
+    sc = opt.score
+    b0, db, b1 = opt.betas
+    rc = _lib.load().ome_treesa(n, arr(C.c_int32, nl), arr(C.c_int32, fl), len(ol), arr(C.c_int32, ol),
+                                len(labels), arr(C.c_double, l2), arr(C.c_int32, init_arr), float(sc.sc_target),
+                                float(sc.sc_weight), float(sc.rw_weight) / max(float(sc.tc_weight), 1e-300),
+                                float(b0), float(db), float(b1), int(opt.niters), int(opt.ntrials),
+                                int(opt.seed) & 0xFFFFFFFFFFFFFFFF, out, cx)
+    if rc != 0:
+        raise ArgumentError(f"ome_treesa failed with status {rc}")
+    res = [(out[2 * k], out[2 * k + 1]) for k in range(n - 1)]
+    return _from_pairs(res, [tuple(ix) for ix in ixs], tuple(iy))
+
+
+def optimize_code(code: AbstractEinsum, size_dict: Dict[Any, int], optimizer=None, simplifier=None,
+                  slicer=None):
     """``optimize_code`` (src/contractionorder.jl:30-32): a NestedEinsum (or a
-    SlicedEinsum when a slicer is given) for the flattened code."""
+    SlicedEinsum when a slicer is given) for the flattened code; optimizer
+    GreedyMethod (default) or TreeSA, simplifier None or MergeVectors()."""
     optimizer = optimizer or GreedyMethod()
     flat = code if isinstance(code, EinCode) else code.flatten()
     ixs = [list(ix) for ix in flat.ixs]
     iy = list(flat.iy)
+    if isinstance(simplifier, MergeVectors) and len(ixs) > 2:
+        keep, groups = _merge_vectors(ixs)
+        if groups and len(keep) >= 2:
+            merged = EinCode([tuple(ixs[t]) for t in keep], tuple(iy))
+            inner = optimize_code(merged, size_dict, optimizer)
+            ne = _expand_merged(inner, keep, groups, ixs)
+            return slice_code(ne, size_dict, slicer) if slicer is not None else ne
     if len(ixs) == 1:
         ne = NestedEinsum([NestedEinsum(0)], EinCode([tuple(ixs[0])], tuple(iy)))
+    elif isinstance(optimizer, TreeSA):
+        ne = _treesa(ixs, iy, size_dict, optimizer)
     else:
         log2sd = {l: math.log2(max(size_dict[l], 1)) for l in flat.uniquelabels()}
         rng = np.random.default_rng(optimizer.seed)
@@ -281,9 +471,44 @@ def optimize_code(code: AbstractEinsum, size_dict: Dict[Any, int], optimizer: Gr
     return ne
 
 
-def slice_code(code: NestedEinsum, size_dict: Dict[Any, int], slicer: GreedySlicer | None = None) -> SlicedEinsum:
-    """``slice_code`` (src/contractionorder.jl:33-35) with the greedy slicer."""
+def _treesa_slice(code: NestedEinsum, size_dict, slicer: TreeSASlicer) -> SlicedEinsum:
+    sd = dict(size_dict)
+    sliced: List[Any] = []
+    ne = code
+    flat = code.flatten()
+    ixs = [list(ix) for ix in flat.ixs]
+    iy = list(flat.iy)
+    target = slicer.score.sc_target
+    for _ in range(len(sd)):
+        tc, sc, _ = tree_complexity(ne, sd)
+        if sc <= target + 1e-9:
+            break
+        best = None
+        for l in flat.uniquelabels():
+            if l in sliced or sd[l] <= 1 or l in iy:
+                continue
+            sd2 = dict(sd)
+            sd2[l] = 1
+            tc2, sc2, _ = tree_complexity(ne, sd2)
+            key = (sc2, tc2 + math.log2(sd[l]))
+            if best is None or key < best[0]:
+                best = (key, l)
+        if best is None:
+            break
+        sliced.append(best[1])
+        sd[best[1]] = 1
+        if len(ixs) > 2:
+            ne = _treesa(ixs, iy, sd, TreeSA(betas=slicer.betas, ntrials=slicer.ntrials, niters=slicer.niters,
+                                             score=slicer.score, seed=slicer.seed + len(sliced)), init=ne)
+    return SlicedEinsum(sliced, ne)
+
+
+def slice_code(code: NestedEinsum, size_dict: Dict[Any, int], slicer=None) -> SlicedEinsum:
+    """``slice_code`` (src/contractionorder.jl:33-35): GreedySlicer (default) or
+    TreeSASlicer."""
     slicer = slicer or GreedySlicer()
+    if isinstance(slicer, TreeSASlicer):
+        return _treesa_slice(code, size_dict, slicer)
     sd = dict(size_dict)
     sliced: List[Any] = []
     labels = code.uniquelabels() if not isinstance(code, NestedEinsum) else \
