@@ -35,6 +35,7 @@ from .engine import (TropicalTensor, cost_and_gradient, einsum, einsum_, einsum_
 from .batch import BatchedEinsum, capture_graph
 from .serve import Job, TNServer, pow2_rescale
 from .distributed import ShardedSlices, allreduce_partial, sharded_einsum, slice_range
+from .autograd import ad_einsum
 from .planner import (GreedyMethod, GreedySlicer, MergeVectors, ScoreFunction, TreeSA, TreeSASlicer,
                       contraction_complexity, flop, label_elimination_order, optimize_code, peak_memory, readjson,
                       slice_code, writejson)
