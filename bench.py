@@ -482,6 +482,19 @@ def main():
         if nw % 8 == 0:
             torch.cuda.synchronize()
     torch.cuda.synchronize()
+    # main kernels per contraction (the library brackets each dispatch's main
+    # kernel with events on its stream when asked): one probe pass
+    import ctypes as C
+    kcount = []
+    fbuf, nbuf, cnt = (C.c_float * 4096)(), (C.c_char_p * 4096)(), C.c_int32()
+    for i, (c, ext) in enumerate(codes):
+        lib.ome_kernel_timing(64)
+        ome.einsum_(c, devs[i], outs[i], True, False, ext)
+        torch.cuda.synchronize()
+        lib.ome_kernel_times(4096, fbuf, nbuf, C.byref(cnt))
+        kcount.append((cnt.value, [nbuf[j].decode() for j in range(cnt.value)]))
+    lib.ome_kernel_timing(0)
+    torch.cuda.synchronize()
     if world > 1:
         dist.barrier()
     n0 = lib.ome_launch_count()
@@ -490,6 +503,25 @@ def main():
         step(k)
     torch.cuda.synchronize()
     launches = lib.ome_launch_count() - n0
+    # the same steps again with the main kernels bracketed by events (they
+    # add a few microseconds per contraction, so the timed steps above run
+    # without them); event pairs are created before this pass
+    nt = args.steps * sum(c for c, _ in kcount)
+    lib.ome_kernel_timing(max(nt, 1))
+    for k in range(args.steps):
+        step()
+    torch.cuda.synchronize()
+    kt = (C.c_float * max(nt, 1))()
+    knames = (C.c_char_p * max(nt, 1))()
+    lib.ome_kernel_times(nt, kt, knames, C.byref(cnt))
+    lib.ome_kernel_timing(0)
+    kernel_ms = [0.0] * len(CASES)   # per contraction: its main kernels' time, averaged over steps
+    if cnt.value == nt:
+        pos = 0
+        for _ in range(args.steps):
+            for i, (c, _) in enumerate(kcount):
+                kernel_ms[i] += sum(kt[pos + j] for j in range(c)) / args.steps
+                pos += c
     cs.__exit__()
     if world > 1:
         dist.barrier()
@@ -523,12 +555,17 @@ def main():
         dist.all_reduce(te, op=dist.ReduceOp.MAX)
     e2e_value = len(CASES) * world / (float(te.item()) / 1e3)
 
-    # roofline of the dominant contraction
+    # roofline of the dominant contraction's main kernel: algorithmic work of
+    # the contraction / that kernel's average event-timed duration in the
+    # timed steps; case_frac is the same over the whole contraction (all its
+    # launches, e.g. the operand packing of the tensor-core GEMM)
     hbm, bf16, src = load_peaks()
     dom = int(np.argmax(per_case))
     name, code, ext, _ = CASES[dom]
     flops, nbytes = case_work(code, ext)
-    dur_s = per_case[dom] / 1e3
+    case_s = per_case[dom] / 1e3
+    dur_s = kernel_ms[dom] / 1e3 if kernel_ms[dom] > 0 else case_s
+    kname = "+".join(kcount[dom][1]) or "all launches"
     nmma = {0: 6, 3: 6, 2: 3}.get(args.prec, 6)   # BF16 MMAs per FP32 product (BF16x6 / BF16x3)
     tc_peak = bf16 / nmma
     t_flop = flops / (tc_peak * 1e12) if flops else 0.0
@@ -537,10 +574,13 @@ def main():
     if t_flop > t_mem:
         roof = {"bound": "tensor", "achieved": flops / dur_s / 1e12, "peak": tc_peak, "unit": "TFLOP/s",
                 "frac": (flops / dur_s / 1e12) / tc_peak, "traffic": traffic,
-                "kernel": name, "peak_source": f"{src} bf16_tflops / {nmma} (FP32-equivalent of BF16x{nmma})"}
+                "kernel": f"{kname} ({name})", "kernel_us": dur_s * 1e6, "case_us": case_s * 1e6,
+                "case_frac": (flops / case_s / 1e12) / tc_peak,
+                "peak_source": f"{src} bf16_tflops / {nmma} (FP32-equivalent of BF16x{nmma})"}
     else:
         roof = {"bound": "hbm", "achieved": nbytes / dur_s / 1e9, "peak": hbm, "unit": "GB/s",
-                "frac": (nbytes / dur_s / 1e9) / hbm, "traffic": traffic, "kernel": name,
+                "frac": (nbytes / dur_s / 1e9) / hbm, "traffic": traffic, "kernel": f"{kname} ({name})",
+                "kernel_us": dur_s * 1e6, "case_us": case_s * 1e6, "case_frac": (nbytes / case_s / 1e9) / hbm,
                 "peak_source": f"{src} hbm_gbs"}
 
     cpu = None
@@ -566,6 +606,9 @@ def main():
     for (nm, code, ext, _), ms in zip(CASES, per_case):
         f, b = case_work(code, ext)
         detail[nm] = {"us": ms * 1e3, "GB/s": b / (ms / 1e3) / 1e9}
+        if kernel_ms[len(detail) - 1] > 0:
+            detail[nm]["main_kernel_us"] = kernel_ms[len(detail) - 1] * 1e3
+            detail[nm]["main_kernel"] = "+".join(kcount[len(detail) - 1][1])
         if f:
             detail[nm]["TFLOP/s"] = f / (ms / 1e3) / 1e12
     if rank == 0:

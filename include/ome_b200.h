@@ -110,6 +110,19 @@ OME_API int ome_device_status(void* stream);
  * stream reports OME_TIMEOUT once; the context stays usable. */
 OME_API int ome_selftest_wait_timeout(void* stream, uint64_t wait_ns);
 
+/* Kernel timing (diagnostic; no counterpart in the reference).  While
+ * enabled, the main kernel of every dispatch (the GEMM of a binary
+ * contraction, the transpose of a permutation, the reduction of a sum, the
+ * index kernel of loop_einsum) is bracketed by CUDA events on its own stream,
+ * without synchronising.  ome_kernel_timing(n) with n > 0 starts the record
+ * (cleared) after creating n event pairs up front, so that recording n
+ * kernels creates no event; 0 stops it.  ome_kernel_times synchronises on the
+ * recorded events
+ * and writes up to `max` durations (ms, launch order) and kernel names
+ * (static strings) to ms / names, and their number to *count. */
+OME_API int ome_kernel_timing(int enable);
+OME_API int ome_kernel_times(int32_t max, float* ms, const char** names, int32_t* count);
+
 /* Message of the last failed call on this host thread ("" if none). */
 OME_API const char* ome_last_error(void);
 

@@ -20,7 +20,8 @@ F32, F64, C32, C64, I64, BOOL, TROP_F32, TROP_F64 = range(8)
 PREC_AUTO, PREC_FP32, PREC_BF16X3, PREC_BF16X6 = range(4)
 
 EXPORTS = [
-    "ome_version", "ome_launch_count", "ome_device_status", "ome_selftest_wait_timeout", "ome_last_error", "ome_ctx_create", "ome_ctx_destroy", "ome_ctx_workspace_bytes",
+    "ome_version", "ome_launch_count", "ome_device_status", "ome_selftest_wait_timeout",
+    "ome_kernel_timing", "ome_kernel_times", "ome_last_error", "ome_ctx_create", "ome_ctx_destroy", "ome_ctx_workspace_bytes",
     "ome_einsum", "ome_loop_einsum", "ome_plan_create", "ome_plan_destroy", "ome_plan_peak_bytes",
     "ome_plan_execute", "ome_plan_gradient", "ome_plan_slice_count", "ome_plan_partial_info",
     "ome_plan_execute_slices", "ome_plan_finish", "ome_reduce_noalloc", "ome_batch_create", "ome_batch_run",
@@ -75,6 +76,9 @@ def load() -> C.CDLL:
         lib.ome_last_error.restype = C.c_char_p
         lib.ome_device_status.argtypes = [P]
         lib.ome_selftest_wait_timeout.argtypes = [P, C.c_uint64]
+        lib.ome_kernel_timing.argtypes = [C.c_int]
+        lib.ome_kernel_times.argtypes = [C.c_int32, C.POINTER(C.c_float), C.POINTER(C.c_char_p),
+                                         C.POINTER(C.c_int32)]
         lib.ome_ctx_create.argtypes = [C.c_int, C.c_size_t, C.POINTER(P)]
         lib.ome_ctx_destroy.argtypes = [P]
         lib.ome_ctx_workspace_bytes.argtypes = [P, C.POINTER(C.c_size_t)]

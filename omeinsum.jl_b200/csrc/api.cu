@@ -682,6 +682,17 @@ int ome_device_status(void* stream) {
   return OME_OK;
 }
 
+int ome_kernel_timing(int enable) {
+  set_kernel_timing(enable);
+  return OME_OK;
+}
+
+int ome_kernel_times(int32_t max, float* ms, const char** names, int32_t* count) {
+  if (max < 0 || (max > 0 && (!ms || !names)) || !count) return set_err(OME_INVALID_ARGUMENT, "NULL argument");
+  *count = read_kernel_times(max, ms, names);
+  return OME_OK;
+}
+
 int ome_selftest_wait_timeout(void* stream, uint64_t wait_ns) {
   return cuda_err(launch_selftest_wait(wait_ns, static_cast<cudaStream_t>(stream)), "self-test kernel");
 }

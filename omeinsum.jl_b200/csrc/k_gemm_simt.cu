@@ -154,6 +154,7 @@ static cudaError_t launch_gemm_simt_t(const GemmArgs& g, cudaStream_t s) {
   if (gm > 0x7fffffff || gn > 65535) return cudaErrorNotSupported;
   const int64_t gl = g.L < 65535 ? g.L : 65535;
   dim3 grid((unsigned)gm, (unsigned)gn, (unsigned)gl);
+  KernelTimer kt(s, "k_gemm_simt");
   k_gemm_simt<A><<<grid, 256, 0, s>>>(g); count_launch();
   return cudaGetLastError();
 }
@@ -231,6 +232,7 @@ cudaError_t launch_gemm_bfast(ome_dtype dt, const GemmArgs& g, cudaStream_t s) {
   const dim3 grid((unsigned)((g.L + 31) / 32), (unsigned)((g.N + 3) / 4), (unsigned)((g.M + 15) / 16));
   cudaError_t e = cudaErrorInvalidValue;
   const bool full = g.M % 16 == 0 && g.N % 4 == 0 && g.L % 32 == 0;
+  KernelTimer kt(s, "k_gemm_bfast");
   OME_DISPATCH(dt, ALG, {
     if (full) k_gemm_bfast<ALG, true><<<grid, 128, 0, s>>>(g);
     else k_gemm_bfast<ALG, false><<<grid, 128, 0, s>>>(g);
@@ -244,6 +246,7 @@ cudaError_t launch_gemm_simt_small_f32(const GemmArgs& g, cudaStream_t s) {
   if (g.M == 0 || g.N == 0 || g.L == 0) return cudaSuccess;
   if (g.M > SimtSmall::BM || g.N > SimtSmall::BN) return cudaErrorNotSupported;
   const int64_t gl = g.L < 65535 ? g.L : 65535;
+  KernelTimer kt(s, "k_gemm_simt");
   k_gemm_simt<AlgF32, SimtSmall><<<dim3(1, 1, (unsigned)gl), 256, 0, s>>>(g);
   count_launch();
   return cudaGetLastError();

@@ -533,6 +533,7 @@ cudaError_t launch_gemm_split(const GemmArgs& g, int nterms, void* workspace, si
   t.S = (int)S;
   t.kchunk = kchunk;
   dim3 grid((unsigned)tm, (unsigned)tn, (unsigned)(g.L * S));
+  KernelTimer kt(s, "k_gemm_bf16x3");
   if (nterms == 2) k_gemm_bf16x3<2><<<grid, NTHREADS, Cfg<2>::SMEM_BYTES, s>>>(t);
   else k_gemm_bf16x3<3><<<grid, NTHREADS, Cfg<3>::SMEM_BYTES, s>>>(t);
   count_launch();
@@ -982,8 +983,11 @@ cudaError_t launch_gemm_packed(const GemmArgs& g, int nterms, void* workspace, s
   t.ksplit = ksplit;
   t.units = F + Rt * S;
   const unsigned grid = (unsigned)std::min<int64_t>(t.units, G);
-  if (nterms == 2) k_gemm_packed<2><<<grid, NTHREADS, Cfg<2>::SMEM_BYTES, s>>>(t);
-  else k_gemm_packed<3><<<grid, NTHREADS, Cfg<3>::SMEM_BYTES, s>>>(t);
+  {
+    KernelTimer kt(s, "k_gemm_packed");
+    if (nterms == 2) k_gemm_packed<2><<<grid, NTHREADS, Cfg<2>::SMEM_BYTES, s>>>(t);
+    else k_gemm_packed<3><<<grid, NTHREADS, Cfg<3>::SMEM_BYTES, s>>>(t);
+  }
   count_launch();
   e = cudaGetLastError();
   if (e != cudaSuccess || Rt == 0) return e;

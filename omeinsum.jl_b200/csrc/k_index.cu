@@ -8,6 +8,8 @@
 //    Repeat (src/unaryrules.jl:44-58, stride-0 input modes) and Identity.
 //  * k_scale, k_acc64*: αβ pre-pass and FP64 cross-slice accumulation.
 #include <string.h>
+#include <mutex>
+#include <vector>
 #include "kernels.h"
 
 namespace ome {
@@ -22,6 +24,68 @@ static int64_t max_offset(int nd, const int64_t* ext, const int64_t* str) {
 static unsigned long long g_launches = 0;
 unsigned long long launch_counter() { return __atomic_load_n(&g_launches, __ATOMIC_RELAXED); }
 void count_launch(int n) { __atomic_fetch_add(&g_launches, (unsigned long long)n, __ATOMIC_RELAXED); }
+
+// ---------------------------------------------------------------------------
+// diagnostic kernel timing
+// ---------------------------------------------------------------------------
+struct TimedKernel {
+  int ev;   // index of its event pair in the pool
+  const char* name;
+};
+static std::mutex g_tmu;
+static bool g_timing = false;
+static std::vector<std::pair<cudaEvent_t, cudaEvent_t>> g_pool;   // created once, reused
+static std::vector<TimedKernel> g_timed;
+static const size_t kMaxTimed = 1 << 16;
+
+static bool grow_pool(size_t n) {
+  while (g_pool.size() < n) {
+    cudaEvent_t b, e;
+    if (cudaEventCreate(&b) != cudaSuccess) { cudaGetLastError(); return false; }
+    if (cudaEventCreate(&e) != cudaSuccess) { cudaEventDestroy(b); cudaGetLastError(); return false; }
+    g_pool.push_back({b, e});
+  }
+  return true;
+}
+
+KernelTimer::KernelTimer(cudaStream_t s_, const char* name_) : s(s_), name(name_), slot(-1) {
+  std::lock_guard<std::mutex> lk(g_tmu);
+  if (!g_timing || g_timed.size() >= kMaxTimed) return;
+  const int idx = (int)g_timed.size();
+  if (!grow_pool((size_t)idx + 1)) return;
+  cudaEventRecord(g_pool[idx].first, s);
+  g_timed.push_back({idx, name});
+  slot = idx;
+}
+
+KernelTimer::~KernelTimer() {
+  if (slot < 0) return;
+  std::lock_guard<std::mutex> lk(g_tmu);
+  if (slot < (int)g_timed.size()) cudaEventRecord(g_pool[g_timed[slot].ev].second, s);
+}
+
+void set_kernel_timing(int n) {
+  std::lock_guard<std::mutex> lk(g_tmu);
+  g_timed.clear();
+  g_timing = n > 0;
+  if (n > 0) grow_pool(std::min((size_t)n, kMaxTimed));
+}
+
+int read_kernel_times(int max, float* ms, const char** names) {
+  std::lock_guard<std::mutex> lk(g_tmu);
+  int n = 0;
+  for (auto& t : g_timed) {
+    if (n >= max) break;
+    float v = -1.f;
+    const auto& ev = g_pool[t.ev];
+    if (cudaEventSynchronize(ev.second) == cudaSuccess) cudaEventElapsedTime(&v, ev.first, ev.second);
+    cudaGetLastError();
+    ms[n] = v;
+    names[n] = t.name;
+    ++n;
+  }
+  return n;
+}
 
 // ---------------------------------------------------------------------------
 // generic loop kernel
@@ -296,6 +360,7 @@ static cudaError_t launch_reduce_contig_t(const LoopArgs& a, bool vec, int64_t r
                      R * a.ext[a.nout] < ((int64_t)1 << 30);
   constexpr int V = 16 / sizeof(typename A::T) > 0 ? 16 / sizeof(typename A::T) : 1;
   const FastDiv chdiv = make_fastdiv((uint32_t)(small ? a.ext[a.nout] / (vec ? V : 1) : 1));
+  KernelTimer kt(s, "k_reduce_contig");
   if (vec) {
     if (small) k_reduce_contig<A, true, int32_t><<<grid, 256, 0, s>>>(a, rchunk, chdiv);
     else k_reduce_contig<A, true, int64_t><<<grid, 256, 0, s>>>(a, rchunk, chdiv);
@@ -338,6 +403,7 @@ static cudaError_t launch_loop_t(const LoopArgs& a, LoopMode mode, int grid, int
 cudaError_t launch_loop(ome_dtype dt, const LoopArgs& a, LoopMode mode, int grid, int block,
                         cudaStream_t s) {
   cudaError_t e = cudaErrorInvalidValue;
+  KernelTimer kt(s, mode == LOOP_BLOCK ? "k_loop_block" : "k_loop_thread");
   OME_DISPATCH(dt, ALG, e = launch_loop_t<ALG>(a, mode, grid, block, s));
   return e;
 }
@@ -668,14 +734,17 @@ static cudaError_t launch_perm_t(const PermArgs& a, int num_sms, cudaStream_t s)
           t.t0 = make_fastdiv((uint32_t)((a.ext[0] + 63) / 64));
           t.tt = make_fastdiv((uint32_t)((a.ext[a.tmode] + pw - 1) / pw));
           const int grid4 = (int)(tiles4 < maxgrid ? tiles4 : maxgrid);
+          KernelTimer kt(s, "k_transpose_v4");
           if (pw == 32) k_transpose_v4<A, 32><<<grid4, 256, 0, s>>>(t);
           else k_transpose_v4<A, 64><<<grid4, 256, 0, s>>>(t);
           count_launch();
           return cudaGetLastError();
         }
       }
+      KernelTimer kt(s, "k_transpose32");
       k_transpose32<A, TY><<<grid, 256, 0, s>>>(t);
     } else {
+      KernelTimer kt(s, "k_transpose");
       k_transpose<A, TY><<<grid, 256, 0, s>>>(a);
     }
     count_launch();
@@ -683,10 +752,12 @@ static cudaError_t launch_perm_t(const PermArgs& a, int num_sms, cudaStream_t s)
              ((uintptr_t)a.x % 16) == 0 && ((uintptr_t)a.y % 16) == 0) {
     const int64_t nb = (a.n / (16 / sizeof(T)) + 255) / 256;
     const int grid = (int)(nb < 1 ? 1 : (nb < maxgrid ? nb : maxgrid));
+    KernelTimer kt(s, "k_copy_vec");
     k_copy_vec<A><<<grid, 256, 0, s>>>(a); count_launch();
   } else {
     const int64_t nb = (a.n + 255) / 256;
     const int grid = (int)(nb < maxgrid ? nb : maxgrid);
+    KernelTimer kt(s, "k_copy");
     k_copy<A><<<grid, 256, 0, s>>>(a); count_launch();
   }
   return cudaGetLastError();

@@ -9,6 +9,19 @@ namespace ome {
 unsigned long long launch_counter();
 void count_launch(int n = 1);
 
+// Diagnostic kernel timing: while enabled (ome_kernel_timing), a KernelTimer
+// records CUDA events around the main kernel of a dispatch on its stream (no
+// synchronisation); ome_kernel_times reads the durations afterwards.
+void set_kernel_timing(int n);
+int read_kernel_times(int max, float* ms, const char** names);
+struct KernelTimer {
+  KernelTimer(cudaStream_t s, const char* name);
+  ~KernelTimer();
+  cudaStream_t s;
+  const char* name;
+  int slot;
+};
+
 enum LoopMode { LOOP_THREAD = 0, LOOP_BLOCK = 1 };
 
 // Generic sum-product (loop_einsum): mode LOOP_THREAD = one thread per output
