@@ -240,6 +240,17 @@ OME_API int ome_treesa(int32_t ntensors, const int32_t* nlabels, const int32_t* 
                        double beta_start, double beta_step, double beta_stop, int32_t niters,
                        int32_t ntrials, uint64_t seed, int32_t* out_tree, double* out_complexity);
 
+/* Greedy pairwise order (OMEinsumContractionOrders' GreedyMethod): contract the
+ * pair of live tensors that share a label (the two smallest when none do)
+ * minimising size(result) - alpha * (size(a) + size(b)); ties at random, or
+ * with temperature > 0 a pair drawn with Boltzmann weights.  nrepeat runs
+ * (seeded from `seed`); the one with the smallest (tc, sc) is written to
+ * out_tree in the ome_treesa format, its (tc, sc, rw) to out_complexity. */
+OME_API int ome_greedy(int32_t ntensors, const int32_t* nlabels, const int32_t* labels, int32_t nout,
+                       const int32_t* out_labels, int32_t nids, const double* log2_sizes, double alpha,
+                       double temperature, int32_t nrepeat, uint64_t seed, int32_t* out_tree,
+                       double* out_complexity);
+
 /* Batched contractions of uneven shapes (one grouped launch) ----------------
  *
  * `count` binary einsums y_i <- sy*y_i + sx*f(x1_i, x2_i) whose label groups

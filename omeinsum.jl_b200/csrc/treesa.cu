@@ -18,8 +18,9 @@
 //          + sc_weight * sum over contractions of max(0, sc - sc_target),
 //    tc = log2 of the product of the extents of the labels a contraction
 //    touches, sc = log2 of its output size, rw = log2 of (inputs + output);
-//  * every trial starts from the given tree and keeps its best tree; the best
-//    trial (lowest cost) is returned.  Trials run on host threads.
+//  * every trial starts from the given tree, ends with sweeps at zero
+//    temperature (improvements only) and keeps its best tree; the best trial
+//    (lowest cost) is returned.  Trials run on host threads.
 #include <math.h>
 #include <stdint.h>
 #include <string.h>
@@ -158,8 +159,12 @@ void anneal(const Net& n, Tree& t, const Score& s, double b0, double db, double 
   best_cost = cost;
   std::vector<int> nodes(NI);
   for (int j = 0; j < NI; ++j) nodes[j] = j;
-  for (double beta = b0; beta <= b1 + 1e-12; beta += db) {
-    for (int it = 0; it < niters; ++it) {
+  // the temperature schedule, then 2 * niters sweeps at zero temperature
+  // (improvements only) so that every trial ends in a local minimum
+  const int nb = (int)floor((b1 - b0) / db + 1e-9) + 1;
+  for (int bi = 0; bi <= nb; ++bi) {
+    const double beta = bi < nb ? b0 + bi * db : INFINITY;
+    for (int it = 0; it < (bi < nb ? niters : 2 * niters); ++it) {
       std::shuffle(nodes.begin(), nodes.end(), rng);
       for (int P : nodes) {
         // candidate rewrites at P: the inner child X = (B, C) and the other child A
@@ -199,7 +204,7 @@ void anneal(const Net& n, Tree& t, const Score& s, double b0, double db, double 
         const double Q2 = Q + new_q - old_q;
         const double cost2 = log2(S2) + s.sc_weight * Q2;
         const double d = cost2 - cost;
-        if (d <= 0 || U(rng) < exp(-beta * d)) {
+        if (d < 0 || (d == 0 && beta < INFINITY) || (beta < INFINITY && U(rng) < exp(-beta * d))) {
           // accepted: fix parent links and the outside sets below the new node
           if (A >= 0) t.parent[A] = X;
           if (B >= 0) t.parent[B] = X;
@@ -341,6 +346,149 @@ int ome_treesa(int32_t ntensors, const int32_t* nlabels, const int32_t* labels, 
     out_complexity[0] = log2(S);
     out_complexity[1] = sc;
     out_complexity[2] = log2(R);
+  }
+  return OME_OK;
+}
+
+// Greedy pairwise order (the GreedyMethod of OMEinsumContractionOrders,
+// restated): repeatedly contract the pair of live tensors that share a label
+// (the two smallest tensors when none do) minimising
+// size(result) - alpha * (size(a) + size(b)); ties broken at random, or, with
+// temperature > 0, a pair drawn with weight exp(-(cost - min) / (temperature *
+// max(|min|, 1))).  nrepeat runs; the one with the smallest (tc, sc) is
+// returned in the ome_treesa tree format.
+int ome_greedy(int32_t ntensors, const int32_t* nlabels, const int32_t* labels, int32_t nout,
+               const int32_t* out_labels, int32_t nids, const double* log2_sizes, double alpha,
+               double temperature, int32_t nrepeat, uint64_t seed, int32_t* out_tree, double* out_complexity) {
+  if (ntensors < 2 || !nlabels || !labels || !log2_sizes || !out_tree) return OME_INVALID_ARGUMENT;
+  if (nids < 1 || nids > 64 * MAXW) return OME_UNSUPPORTED;
+  Net n;
+  n.T = ntensors;
+  n.L = nids;
+  n.W = (nids + 63) / 64;
+  n.lsz.assign(log2_sizes, log2_sizes + nids);
+  n.u = n.lsz[0];
+  for (double v : n.lsz) n.uniform = n.uniform && v == n.u;
+  n.leaf.resize(ntensors);
+  int64_t pos = 0;
+  for (int t = 0; t < ntensors; ++t) {
+    memset(&n.leaf[t], 0, sizeof(Bits));
+    for (int k = 0; k < nlabels[t]; ++k) {
+      const int l = labels[pos++];
+      if (l < 0 || l >= nids) return OME_INVALID_ARGUMENT;
+      n.leaf[t].w[l >> 6] |= 1ull << (l & 63);
+    }
+  }
+  memset(&n.out, 0, sizeof(Bits));
+  for (int k = 0; k < nout; ++k) {
+    const int l = out_labels[k];
+    if (l < 0 || l >= nids) return OME_INVALID_ARGUMENT;
+    n.out.w[l >> 6] |= 1ull << (l & 63);
+  }
+  const int NI = ntensors - 1;
+  std::mt19937_64 rng(seed);
+  std::uniform_real_distribution<double> U(0.0, 1.0);
+  std::vector<int32_t> best_tree;
+  double best_tc = INFINITY, best_sc = INFINITY, best_rw = 0;
+  for (int rep = 0; rep < std::max(1, nrepeat); ++rep) {
+    // live slots: label bitset, tree ref; per-label number of live slots holding it
+    std::vector<Bits> lab(n.leaf);
+    std::vector<int> ref(ntensors), alive(ntensors, 1);
+    for (int t = 0; t < ntensors; ++t) ref[t] = -t - 1;
+    std::vector<int> cnt(nids, 0);
+    for (int t = 0; t < ntensors; ++t)
+      for (int l = 0; l < nids; ++l)
+        if (lab[t].w[l >> 6] >> (l & 63) & 1) ++cnt[l];
+    std::vector<int32_t> tree;
+    tree.reserve(2 * NI);
+    double S = 0, R = 0, sc = 0;
+    auto result = [&](int a, int b) {
+      Bits u = bor(lab[a], lab[b], n.W), r{};
+      for (int i = 0; i < n.W; ++i) {
+        uint64_t x = u.w[i];
+        while (x) {
+          const int k = __builtin_ctzll(x);
+          const int l = i * 64 + k;
+          const int inside = (int)(lab[a].w[i] >> k & 1) + (int)(lab[b].w[i] >> k & 1);
+          if ((n.out.w[i] >> k & 1) || cnt[l] > inside) r.w[i] |= 1ull << k;
+          x &= x - 1;
+        }
+      }
+      return r;
+    };
+    int live = ntensors;
+    while (live > 1) {
+      // candidate pairs: live slots sharing a label
+      std::vector<std::pair<int, int>> cand;
+      for (int a = 0; a < ntensors; ++a) {
+        if (!alive[a]) continue;
+        for (int b = a + 1; b < ntensors; ++b) {
+          if (!alive[b]) continue;
+          bool share = false;
+          for (int i = 0; i < n.W && !share; ++i) share = (lab[a].w[i] & lab[b].w[i]) != 0;
+          if (share) cand.push_back({a, b});
+        }
+      }
+      if (cand.empty()) {
+        int s1 = -1, s2 = -1;
+        for (int a = 0; a < ntensors; ++a) {
+          if (!alive[a]) continue;
+          if (s1 < 0 || lsum(n, lab[a]) < lsum(n, lab[s1])) { s2 = s1; s1 = a; }
+          else if (s2 < 0 || lsum(n, lab[a]) < lsum(n, lab[s2])) s2 = a;
+        }
+        cand.push_back({std::min(s1, s2), std::max(s1, s2)});
+      }
+      std::vector<double> cost(cand.size());
+      double cmin = INFINITY;
+      for (size_t i = 0; i < cand.size(); ++i) {
+        const int a = cand[i].first, b = cand[i].second;
+        cost[i] = exp2(lsum(n, result(a, b))) - alpha * (exp2(lsum(n, lab[a])) + exp2(lsum(n, lab[b])));
+        cmin = std::min(cmin, cost[i]);
+      }
+      size_t pick = 0;
+      if (temperature > 0) {
+        double tot = 0;
+        std::vector<double> w(cand.size());
+        for (size_t i = 0; i < cand.size(); ++i) tot += (w[i] = exp(-(cost[i] - cmin) / (temperature * std::max(fabs(cmin), 1.0))));
+        double x = U(rng) * tot;
+        for (pick = 0; pick + 1 < cand.size() && x >= w[pick]; ++pick) x -= w[pick];
+      } else {
+        std::vector<size_t> ties;
+        for (size_t i = 0; i < cand.size(); ++i)
+          if (cost[i] == cmin) ties.push_back(i);
+        pick = ties[(size_t)(U(rng) * ties.size()) % ties.size()];
+      }
+      const int a = cand[pick].first, b = cand[pick].second;
+      const Bits r = result(a, b);
+      const double tcn = lsum(n, bor(lab[a], lab[b], n.W)), scn = lsum(n, r);
+      const double sa = lsum(n, lab[a]), sb = lsum(n, lab[b]);
+      S += exp2(tcn);
+      R += exp2(sa) + exp2(sb) + exp2(scn);
+      sc = std::max(sc, scn);
+      tree.push_back(ref[a]);
+      tree.push_back(ref[b]);
+      for (int l = 0; l < nids; ++l) {
+        cnt[l] -= (int)(lab[a].w[l >> 6] >> (l & 63) & 1) + (int)(lab[b].w[l >> 6] >> (l & 63) & 1);
+        cnt[l] += (int)(r.w[l >> 6] >> (l & 63) & 1);
+      }
+      lab[a] = r;
+      ref[a] = (int)(tree.size() / 2) - 1;
+      alive[b] = 0;
+      --live;
+    }
+    const double tc = log2(S);
+    if (tc < best_tc - 1e-12 || (fabs(tc - best_tc) <= 1e-12 && sc < best_sc)) {
+      best_tc = tc;
+      best_sc = sc;
+      best_rw = log2(R);
+      best_tree = tree;
+    }
+  }
+  for (int i = 0; i < 2 * NI; ++i) out_tree[i] = best_tree[i];
+  if (out_complexity) {
+    out_complexity[0] = best_tc;
+    out_complexity[1] = best_sc;
+    out_complexity[2] = best_rw;
   }
   return OME_OK;
 }

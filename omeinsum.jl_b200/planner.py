@@ -1,5 +1,6 @@
-"""Contraction-order planning on the host: a greedy order, a greedy slicer and
-the complexity measures the reference re-exports from OMEinsumContractionOrders
+"""Contraction-order planning on the host: greedy and simulated-annealing
+orders (native searches, ``ome_greedy`` / ``ome_treesa``), slicers and the
+complexity measures the reference re-exports from OMEinsumContractionOrders
 (src/contractionorder.jl:30-51).
 
 OMEinsumContractionOrders (compat 1.1, not vendored with the reference) is an
@@ -60,7 +61,9 @@ class TreeSA:
     TreeSA; the search runs natively, ``ome_treesa``).  ``betas`` = (start,
     step, stop) of the inverse temperature (Julia's 0.01:0.05:15), ``niters``
     sweeps per temperature, ``ntrials`` independent trials from the
-    ``initializer`` tree ("greedy" or "random")."""
+    ``initializer`` tree ("greedy" or "random").  Space complexity above
+    min(score.sc_target, the initial tree's) is penalised, so the search does
+    not trade a larger peak intermediate for time."""
 
     betas: Tuple[float, float, float] = (0.01, 0.05, 15.0)
     ntrials: int = 10
@@ -94,93 +97,6 @@ class MergeVectors:
 
 def _log2sz(labels, log2sd) -> float:
     return float(sum(log2sd[l] for l in labels))
-
-
-def _greedy_once(ixs: List[List[Any]], iy: List[Any], log2sd: Dict[Any, float], rng, alpha, temperature):
-    """One greedy pass; returns a list of (i, j) merges over tensor slots."""
-    n = len(ixs)
-    tensors: Dict[int, Tuple[Any, ...]] = {i: tuple(dict.fromkeys(ix)) for i, ix in enumerate(ixs)}
-    where: Dict[Any, set] = {}
-    for i, ix in tensors.items():
-        for l in ix:
-            where.setdefault(l, set()).add(i)
-    out = set(iy)
-    nodes: Dict[int, Any] = {i: i for i in range(n)}  # slot -> tree (leaf index or tuple)
-    labels_of: Dict[int, Tuple[Any, ...]] = dict(tensors)
-    next_id = n
-
-    def result_labels(a, b):
-        la, lb = labels_of[a], labels_of[b]
-        res = []
-        for l in la + tuple(x for x in lb if x not in la):
-            others = where[l] - {a, b}
-            if l in out or others:
-                res.append(l)
-        return tuple(res)
-
-    def cost(a, b):
-        r = result_labels(a, b)
-        sr = 2.0 ** _log2sz(r, log2sd)
-        sa = 2.0 ** _log2sz(labels_of[a], log2sd)
-        sb = 2.0 ** _log2sz(labels_of[b], log2sd)
-        return sr - alpha * (sa + sb)
-
-    while len(labels_of) > 1:
-        cand = set()
-        for l, ts in where.items():
-            ts = sorted(ts)
-            for x in range(len(ts)):
-                for y in range(x + 1, len(ts)):
-                    cand.add((ts[x], ts[y]))
-        if not cand:
-            ks = sorted(labels_of, key=lambda k: _log2sz(labels_of[k], log2sd))
-            cand = {(min(ks[0], ks[1]), max(ks[0], ks[1]))}
-        cand = sorted(cand)
-        costs = np.array([cost(a, b) for a, b in cand])
-        if temperature > 0:
-            w = np.exp(-(costs - costs.min()) / (temperature * max(abs(costs.min()), 1.0)))
-            k = rng.choice(len(cand), p=w / w.sum())
-        else:
-            best = np.flatnonzero(costs == costs.min())
-            k = int(rng.choice(best))
-        a, b = cand[k]
-        r = result_labels(a, b)
-        nid = next_id
-        next_id += 1
-        nodes[nid] = (nodes.pop(a), nodes.pop(b), labels_of[a], labels_of[b], r)
-        for l in labels_of[a]:
-            where[l].discard(a)
-        for l in labels_of[b]:
-            where[l].discard(b)
-        del labels_of[a]
-        del labels_of[b]
-        labels_of[nid] = r
-        for l in r:
-            where.setdefault(l, set()).add(nid)
-        for l in list(where):
-            if not where[l]:
-                del where[l]
-    (root_slot,) = labels_of.keys()
-    return nodes[root_slot], labels_of[root_slot]
-
-
-def _to_nested(t, iy) -> NestedEinsum:
-    """Build a NestedEinsum from the greedy merge tree; the root contracts to iy."""
-    if isinstance(t, int):
-        raise ValueError("single leaf")
-
-    def rec(t, out):
-        a, b, la, lb, _ = t
-        args, ixs = [], []
-        for sub, lab in ((a, la), (b, lb)):
-            if isinstance(sub, int):
-                args.append(NestedEinsum(sub))
-            else:
-                args.append(rec(sub, lab))
-            ixs.append(tuple(lab))
-        return NestedEinsum(args, EinCode(ixs, tuple(out)))
-
-    return rec(t, iy)
 
 
 def tree_complexity(ne: NestedEinsum, size_dict) -> Tuple[float, float, float]:
@@ -389,13 +305,38 @@ def _expand_merged(ne: NestedEinsum, keep: List[int], groups: Dict[int, List[int
     return rec(ne)
 
 
+def _net(ixs: List[List[Any]], iy: List[Any], size_dict):
+    """The network as the native planners take it: label ids, per-tensor label
+    counts and ids, output ids, log2 extents."""
+    import ctypes as C
+    labels = list(dict.fromkeys([l for ix in ixs for l in ix] + list(iy)))
+    lid = {l: i for i, l in enumerate(labels)}
+    arr = lambda T, v: (T * max(len(v), 1))(*v)
+    return (arr(C.c_int32, [len(ix) for ix in ixs]), arr(C.c_int32, [lid[l] for ix in ixs for l in ix]),
+            len([l for l in iy if l in lid]), arr(C.c_int32, [lid[l] for l in iy if l in lid]), len(labels),
+            arr(C.c_double, [math.log2(max(size_dict[l], 1)) for l in labels]))
+
+
+def _greedy(ixs: List[List[Any]], iy: List[Any], size_dict, opt: GreedyMethod) -> NestedEinsum:
+    """GreedyMethod through the native search (``ome_greedy``)."""
+    import ctypes as C
+
+    from . import _lib
+    n = len(ixs)
+    nl, fl, no, ol, nids, l2 = _net(ixs, iy, size_dict)
+    out = (C.c_int32 * (2 * (n - 1)))()
+    rc = _lib.load().ome_greedy(n, nl, fl, no, ol, nids, l2, float(opt.alpha), float(opt.temperature),
+                                int(opt.nrepeat), int(opt.seed) & 0xFFFFFFFFFFFFFFFF, out, None)
+    if rc != 0:
+        raise ArgumentError(f"ome_greedy failed with status {rc}")
+    return _from_pairs([(out[2 * k], out[2 * k + 1]) for k in range(n - 1)], [tuple(ix) for ix in ixs], tuple(iy))
+
+
 def _treesa(ixs: List[List[Any]], iy: List[Any], size_dict, opt: TreeSA, init: NestedEinsum | None = None):
     """Run ome_treesa on the network and return the best tree as a NestedEinsum."""
     import ctypes as C
 
     from . import _lib
-    labels = list(dict.fromkeys([l for ix in ixs for l in ix] + list(iy)))
-    lid = {l: i for i, l in enumerate(labels)}
     n = len(ixs)
     if init is None:
         if opt.initializer == "random":
@@ -408,23 +349,19 @@ def _treesa(ixs: List[List[Any]], iy: List[Any], size_dict, opt: TreeSA, init: N
                 pairs.append((a, b))
                 slots = [x for k, x in enumerate(slots) if k not in (i, j)] + [len(pairs) - 1]
         else:
-            g = optimize_code(EinCode([tuple(ix) for ix in ixs], tuple(iy)), size_dict,
-                              GreedyMethod(nrepeat=1, seed=opt.seed))
-            pairs = _post_order_pairs(g)
+            pairs = _post_order_pairs(_greedy(ixs, iy, size_dict, GreedyMethod(nrepeat=1, seed=opt.seed)))
     else:
         pairs = _post_order_pairs(init)
-    arr = lambda T, v: (T * max(len(v), 1))(*v)
-    nl = [len(ix) for ix in ixs]
-    fl = [lid[l] for ix in ixs for l in ix]
-    ol = [lid[l] for l in iy if l in lid]
-    l2 = [math.log2(max(size_dict[l], 1)) for l in labels]
-    init_arr = [x for p in pairs for x in p]
+    # never accept a larger peak intermediate than the starting tree's: the
+    # effective target is min(score.sc_target, sc of the initial tree)
+    start_sc = tree_complexity(_from_pairs(pairs, [tuple(ix) for ix in ixs], tuple(iy)), size_dict)[1]
+    nl, fl, no, ol, nids, l2 = _net(ixs, iy, size_dict)
+    init_arr = (C.c_int32 * (2 * (n - 1)))(*[x for p in pairs for x in p])
     out = (C.c_int32 * (2 * (n - 1)))()
     cx = (C.c_double * 3)()
     sc = opt.score
     b0, db, b1 = opt.betas
-    rc = _lib.load().ome_treesa(n, arr(C.c_int32, nl), arr(C.c_int32, fl), len(ol), arr(C.c_int32, ol),
-                                len(labels), arr(C.c_double, l2), arr(C.c_int32, init_arr), float(sc.sc_target),
+    rc = _lib.load().ome_treesa(n, nl, fl, no, ol, nids, l2, init_arr, float(min(sc.sc_target, start_sc)),
                                 float(sc.sc_weight), float(sc.rw_weight) / max(float(sc.tc_weight), 1e-300),
                                 float(b0), float(db), float(b1), int(opt.niters), int(opt.ntrials),
                                 int(opt.seed) & 0xFFFFFFFFFFFFFFFF, out, cx)
@@ -455,17 +392,7 @@ def optimize_code(code: AbstractEinsum, size_dict: Dict[Any, int], optimizer=Non
     elif isinstance(optimizer, TreeSA):
         ne = _treesa(ixs, iy, size_dict, optimizer)
     else:
-        log2sd = {l: math.log2(max(size_dict[l], 1)) for l in flat.uniquelabels()}
-        rng = np.random.default_rng(optimizer.seed)
-        best = None
-        for _ in range(max(1, optimizer.nrepeat)):
-            t, _ = _greedy_once(ixs, iy, log2sd, rng, optimizer.alpha, optimizer.temperature)
-            ne = _to_nested(t, iy)
-            tc = tree_complexity(ne, size_dict)
-            key = (tc[0], tc[1])
-            if best is None or key < best[0]:
-                best = (key, ne)
-        ne = best[1]
+        ne = _greedy(ixs, iy, size_dict, optimizer)
     if slicer is not None:
         return slice_code(ne, size_dict, slicer)
     return ne
