@@ -251,6 +251,18 @@ OME_API int ome_greedy(int32_t ntensors, const int32_t* nlabels, const int32_t* 
                        double temperature, int32_t nrepeat, uint64_t seed, int32_t* out_tree,
                        double* out_complexity);
 
+/* Greedy slicer (the slicing loop of src/slicing.jl's SlicedEinsum with
+ * OMEinsumContractionOrders' slicers as the reference uses them): slice, one
+ * at a time, the label whose removal gives the smallest (space complexity,
+ * time complexity + its log2 extent) until the largest intermediate of
+ * `tree` (ome_treesa format) has at most 2^sc_target elements or max_slices
+ * labels are sliced; `forbidden` (NULL or nids flags) excludes labels.  The
+ * sliced label ids go to out_sliced in order, their number to *out_count. */
+OME_API int ome_slice_greedy(int32_t ntensors, const int32_t* nlabels, const int32_t* labels, int32_t nout,
+                             const int32_t* out_labels, int32_t nids, const double* log2_sizes,
+                             const int32_t* tree, double sc_target, int32_t max_slices,
+                             const int32_t* forbidden, int32_t* out_sliced, int32_t* out_count);
+
 /* Batched contractions of uneven shapes (one grouped launch) ----------------
  *
  * `count` binary einsums y_i <- sy*y_i + sx*f(x1_i, x2_i) whose label groups

@@ -25,7 +25,7 @@ EXPORTS = [
     "ome_einsum", "ome_loop_einsum", "ome_plan_create", "ome_plan_destroy", "ome_plan_peak_bytes",
     "ome_plan_execute", "ome_plan_gradient", "ome_plan_slice_count", "ome_plan_partial_info",
     "ome_plan_execute_slices", "ome_plan_finish", "ome_reduce_noalloc", "ome_batch_create", "ome_batch_run",
-    "ome_batch_info", "ome_batch_destroy", "ome_treesa", "ome_greedy",
+    "ome_batch_info", "ome_batch_destroy", "ome_treesa", "ome_greedy", "ome_slice_greedy",
 ]
 
 
@@ -104,6 +104,8 @@ def load() -> C.CDLL:
         lib.ome_treesa.argtypes = [C.c_int32, i32p, i32p, C.c_int32, i32p, C.c_int32, dp, i32p, C.c_double,
                                    C.c_double, C.c_double, C.c_double, C.c_double, C.c_double, C.c_int32,
                                    C.c_int32, C.c_uint64, i32p, dp]
+        lib.ome_slice_greedy.argtypes = [C.c_int32, i32p, i32p, C.c_int32, i32p, C.c_int32, dp, i32p, C.c_double,
+                                         C.c_int32, i32p, i32p, i32p]
         lib.ome_greedy.argtypes = [C.c_int32, i32p, i32p, C.c_int32, i32p, C.c_int32, dp, C.c_double, C.c_double,
                                    C.c_int32, C.c_uint64, i32p, dp]
         for f in EXPORTS:

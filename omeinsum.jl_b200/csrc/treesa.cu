@@ -350,6 +350,108 @@ int ome_treesa(int32_t ntensors, const int32_t* nlabels, const int32_t* labels, 
   return OME_OK;
 }
 
+// Greedy slicer: given a tree (ome_treesa format), repeatedly slice the label
+// (extent set to 1) that gives the smallest (space complexity, time
+// complexity + log2 extent of the label) until the largest intermediate fits
+// 2^sc_target elements or max_slices labels are sliced.  Node label sets are
+// computed once; a candidate only re-sums costs.
+int ome_slice_greedy(int32_t ntensors, const int32_t* nlabels, const int32_t* labels, int32_t nout,
+                     const int32_t* out_labels, int32_t nids, const double* log2_sizes, const int32_t* tree,
+                     double sc_target, int32_t max_slices, const int32_t* forbidden, int32_t* out_sliced,
+                     int32_t* out_count) {
+  if (ntensors < 2 || !nlabels || !labels || !log2_sizes || !tree || !out_sliced || !out_count)
+    return OME_INVALID_ARGUMENT;
+  if (nids < 1 || nids > 64 * MAXW) return OME_UNSUPPORTED;
+  Net n;
+  n.T = ntensors;
+  n.L = nids;
+  n.W = (nids + 63) / 64;
+  n.lsz.assign(log2_sizes, log2_sizes + nids);
+  n.uniform = false;
+  n.leaf.resize(ntensors);
+  int64_t pos = 0;
+  for (int t = 0; t < ntensors; ++t) {
+    memset(&n.leaf[t], 0, sizeof(Bits));
+    for (int k = 0; k < nlabels[t]; ++k) {
+      const int l = labels[pos++];
+      if (l < 0 || l >= nids) return OME_INVALID_ARGUMENT;
+      n.leaf[t].w[l >> 6] |= 1ull << (l & 63);
+    }
+  }
+  memset(&n.out, 0, sizeof(Bits));
+  for (int k = 0; k < nout; ++k) {
+    const int l = out_labels[k];
+    if (l < 0 || l >= nids) return OME_INVALID_ARGUMENT;
+    n.out.w[l >> 6] |= 1ull << (l & 63);
+  }
+  const int NI = ntensors - 1;
+  Tree t;
+  t.left.resize(NI); t.right.resize(NI); t.parent.assign(NI, -1);
+  t.sub.resize(NI); t.outside.resize(NI); t.outb.resize(NI);
+  t.tc.resize(NI); t.sc.resize(NI); t.rw.resize(NI);
+  std::vector<int> used(ntensors, 0);
+  for (int j = 0; j < NI; ++j)
+    for (int side = 0; side < 2; ++side) {
+      const int r = tree[2 * j + side];
+      if (r >= 0) {
+        if (r >= j || t.parent[r] != -1) return OME_INVALID_ARGUMENT;
+        t.parent[r] = j;
+      } else {
+        const int leaf = -r - 1;
+        if (leaf >= ntensors || used[leaf]) return OME_INVALID_ARGUMENT;
+        used[leaf] = 1;
+      }
+      (side ? t.right : t.left)[j] = r;
+    }
+  for (int x = 0; x < ntensors; ++x)
+    if (!used[x]) return OME_INVALID_ARGUMENT;
+  t.root = NI - 1;
+  recompute(n, t);
+  // per node: the labels it touches (children's outputs) and its output
+  std::vector<Bits> touch(NI);
+  Bits any{};
+  for (int j = 0; j < NI; ++j) {
+    touch[j] = bor(out_of(n, t, t.left[j]), out_of(n, t, t.right[j]), n.W);
+    any = bor(any, touch[j], n.W);
+  }
+  auto eval = [&](double& sc, double& tc) {
+    double S = 0;
+    sc = 0;
+    for (int j = 0; j < NI; ++j) {
+      S += exp2(lsum(n, touch[j]));
+      sc = std::max(sc, lsum(n, t.outb[j]));
+    }
+    tc = log2(S);
+  };
+  int cnt = 0;
+  while (cnt < max_slices) {
+    double sc, tc;
+    eval(sc, tc);
+    if (sc <= sc_target + 1e-9) break;
+    int best = -1;
+    double bsc = INFINITY, bkey = INFINITY;
+    for (int l = 0; l < nids; ++l) {
+      if (!(any.w[l >> 6] >> (l & 63) & 1) || n.lsz[l] <= 0 || (forbidden && forbidden[l])) continue;
+      const double keep = n.lsz[l];
+      n.lsz[l] = 0;
+      double sc2, tc2;
+      eval(sc2, tc2);
+      n.lsz[l] = keep;
+      const double key = tc2 + keep;
+      if (sc2 < bsc - 1e-12 || (fabs(sc2 - bsc) <= 1e-12 && key < bkey - 1e-12)) {
+        bsc = sc2;
+        bkey = key;
+        best = l;
+      }
+    }
+    if (best < 0) break;
+    n.lsz[best] = 0;
+    out_sliced[cnt++] = best;
+  }
+  *out_count = cnt;
+  return OME_OK;
+}
+
 // Greedy pairwise order (the GreedyMethod of OMEinsumContractionOrders,
 // restated): repeatedly contract the pair of live tensors that share a label
 // (the two smallest tensors when none do) minimising

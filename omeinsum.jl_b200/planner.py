@@ -398,6 +398,44 @@ def optimize_code(code: AbstractEinsum, size_dict: Dict[Any, int], optimizer=Non
     return ne
 
 
+def _native_slice(code: NestedEinsum, size_dict, sc_target: float, max_slices: int, forbid=()):
+    """Labels to slice, chosen by ``ome_slice_greedy``; None when the tree is
+    not one the native search describes exactly (a node with other than two
+    children, or intermediates that keep more labels than their leaves need)."""
+    import ctypes as C
+
+    from . import _lib
+    try:
+        pairs = _post_order_pairs(code)
+    except ArgumentError:
+        return None
+    flat = code.flatten()
+    ixs = [list(ix) for ix in flat.ixs]
+    iy = list(flat.iy)
+    if len(ixs) < 2:
+        return []
+    canon = _from_pairs(pairs, [tuple(ix) for ix in ixs], tuple(iy))
+
+    def same(a, b):
+        if a.isleaf or b.isleaf:
+            return a.isleaf and b.isleaf
+        return set(a.eins.iy) == set(b.eins.iy) and all(same(x, y) for x, y in zip(a.args, b.args))
+
+    if not same(code, canon):
+        return None
+    labels = list(dict.fromkeys([l for ix in ixs for l in ix] + iy))
+    nl, fl, no, ol, nids, l2 = _net(ixs, iy, size_dict)
+    tree = (C.c_int32 * (2 * len(pairs)))(*[x for p in pairs for x in p])
+    fb = (C.c_int32 * nids)(*[1 if l in forbid else 0 for l in labels])
+    out = (C.c_int32 * nids)()
+    cnt = C.c_int32()
+    rc = _lib.load().ome_slice_greedy(len(ixs), nl, fl, no, ol, nids, l2, tree, float(sc_target), int(max_slices),
+                                      fb, out, C.byref(cnt))
+    if rc != 0:
+        raise ArgumentError(f"ome_slice_greedy failed with status {rc}")
+    return [labels[out[k]] for k in range(cnt.value)]
+
+
 def _treesa_slice(code: NestedEinsum, size_dict, slicer: TreeSASlicer) -> SlicedEinsum:
     sd = dict(size_dict)
     sliced: List[Any] = []
@@ -410,20 +448,23 @@ def _treesa_slice(code: NestedEinsum, size_dict, slicer: TreeSASlicer) -> Sliced
         tc, sc, _ = tree_complexity(ne, sd)
         if sc <= target + 1e-9:
             break
-        best = None
-        for l in flat.uniquelabels():
-            if l in sliced or sd[l] <= 1 or l in iy:
-                continue
-            sd2 = dict(sd)
-            sd2[l] = 1
-            tc2, sc2, _ = tree_complexity(ne, sd2)
-            key = (sc2, tc2 + math.log2(sd[l]))
-            if best is None or key < best[0]:
-                best = (key, l)
-        if best is None:
+        pick = _native_slice(ne, sd, target, 1, forbid=set(iy))
+        if pick is None:   # a tree the native search does not describe
+            best = None
+            for l in flat.uniquelabels():
+                if l in sliced or sd[l] <= 1 or l in iy:
+                    continue
+                sd2 = dict(sd)
+                sd2[l] = 1
+                tc2, sc2, _ = tree_complexity(ne, sd2)
+                key = (sc2, tc2 + math.log2(sd[l]))
+                if best is None or key < best[0]:
+                    best = (key, l)
+            pick = [] if best is None else [best[1]]
+        if not pick:
             break
-        sliced.append(best[1])
-        sd[best[1]] = 1
+        sliced.append(pick[0])
+        sd[pick[0]] = 1
         if len(ixs) > 2:
             ne = _treesa(ixs, iy, sd, TreeSA(betas=slicer.betas, ntrials=slicer.ntrials, niters=slicer.niters,
                                              score=slicer.score, seed=slicer.seed + len(sliced)), init=ne)
@@ -436,6 +477,10 @@ def slice_code(code: NestedEinsum, size_dict: Dict[Any, int], slicer=None) -> Sl
     slicer = slicer or GreedySlicer()
     if isinstance(slicer, TreeSASlicer):
         return _treesa_slice(code, size_dict, slicer)
+    picked = _native_slice(code, size_dict, slicer.sc_target, len(size_dict))
+    if picked is not None:
+        return SlicedEinsum(picked, code)
+    # a tree with n-ary nodes or wider intermediates: the same search on the tree itself
     sd = dict(size_dict)
     sliced: List[Any] = []
     labels = code.uniquelabels() if not isinstance(code, NestedEinsum) else \
