@@ -128,7 +128,11 @@ OME_API const char* ome_last_error(void);
 
 /* Create a context on `device` with a device workspace of `workspace_bytes`
  * (intermediates of plans and scratch of single calls).  Replaces the per-
- * intermediate CUDA.jl allocations (ext/CUDAExt.jl:34-47, :129-131). */
+ * intermediate CUDA.jl allocations (ext/CUDAExt.jl:34-47, :129-131).
+ * A large FP32 GEMM whose BF16 operand terms do not fit the workspace puts
+ * them in a second buffer that the context grows on demand (not during
+ * stream capture, at most a quarter of the free device memory; growing
+ * synchronises the device) and frees in ome_ctx_destroy. */
 OME_API int ome_ctx_create(int device, size_t workspace_bytes, ome_ctx** out);
 OME_API int ome_ctx_destroy(ome_ctx* ctx);
 OME_API int ome_ctx_workspace_bytes(const ome_ctx* ctx, size_t* out);

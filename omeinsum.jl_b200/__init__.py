@@ -16,7 +16,8 @@ Public API (names follow OMEinsum.jl; ``!`` becomes a trailing ``_``):
   ``GreedySlicer``, ``contraction_complexity``, ``flop``, ``peak_memory``,
   ``label_elimination_order``, ``writejson``, ``readjson``;
 * batching: ``BatchedEinsum`` (one grouped launch for many contractions of
-  uneven shapes), ``capture_graph``;
+  uneven shapes), ``capture_graph``, ``einsum_many`` (independent
+  contractions of host tensors with uploads and downloads overlapped);
 * serving: ``TNServer`` / ``Job`` (continuous batching of whole networks by
   peak workspace bytes, p50/p99 latency);
 * element types: torch float32/float64/complex64/complex128/int64/bool and
@@ -30,8 +31,8 @@ from .backends import (B200Backend, CuTensorBackend, DefaultBackend, EinsumBacke
 from .core import (AbstractEinsum, DynamicEinCode, DynamicNestedEinsum, EinCode, NestedEinsum, SlicedEinsum,
                    StaticEinCode, StaticNestedEinsum, drop_slicedim, ein, flatten, get_size_dict, getixsv, getiyv,
                    parse_nested, slice_iterator, uniformsize)
-from .engine import (TropicalTensor, cost_and_gradient, einsum, einsum_, einsum_grad, get_output_array,
-                     loop_einsum, loop_einsum_, promote_dtype)
+from .engine import (TropicalTensor, cost_and_gradient, einsum, einsum_, einsum_grad, einsum_many,
+                     get_output_array, loop_einsum, loop_einsum_, promote_dtype)
 from .batch import BatchedEinsum, capture_graph
 from .serve import Job, TNServer, pow2_rescale
 from .distributed import ShardedSlices, allreduce_partial, sharded_einsum, slice_range

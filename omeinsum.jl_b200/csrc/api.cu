@@ -474,6 +474,42 @@ static int gemm_kernel_choice(const GemmArgs& g) {
   return g.M >= 256 && g.N >= 256 && g.K >= 512 && flops >= 1e9 ? 1 : 0;
 }
 
+// Scratch of `need` bytes for a packed GEMM whose operands do not fit the
+// workspace: the context's overflow buffer, grown (64 MiB granules) when it
+// is smaller, but never during stream capture and never past a quarter of
+// the free device memory.  Growing waits for the device (the old buffer may
+// still be read by earlier launches).  nullptr: use the in-kernel-converter
+// GEMM instead.
+static void* overflow_scratch(ome_ctx* ctx, size_t need, cudaStream_t s) {
+  if (need <= ctx->ovf_bytes) return ctx->ovf;
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(s, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone) {
+    cudaGetLastError();
+    return nullptr;
+  }
+  size_t fr = 0, tot = 0;
+  if (cudaMemGetInfo(&fr, &tot) != cudaSuccess) {
+    cudaGetLastError();
+    return nullptr;
+  }
+  const size_t gran = (size_t)64 << 20;
+  const size_t want = (need + gran - 1) / gran * gran;
+  if (want > (fr + ctx->ovf_bytes) / 4) return nullptr;
+  if (ctx->ovf) {
+    if (cudaDeviceSynchronize() != cudaSuccess) return nullptr;
+    cudaFree(ctx->ovf);
+    ctx->ovf = nullptr;
+    ctx->ovf_bytes = 0;
+  }
+  if (cudaMalloc(&ctx->ovf, want) != cudaSuccess) {
+    cudaGetLastError();
+    ctx->ovf = nullptr;
+    return nullptr;
+  }
+  ctx->ovf_bytes = want;
+  return ctx->ovf;
+}
+
 static int run_binary(ome_ctx* ctx, cudaStream_t s, ome_dtype dt, HView x1, HView x2, const HView& yu,
                       const Scalar& sx, const Scalar& sy, bool sy_zero, int prec) {
   OME_CK(reduce_dangling(ctx, s, dt, x1, x2, yu));
@@ -566,7 +602,14 @@ static int run_binary(ome_ctx* ctx, cudaStream_t s, ome_dtype dt, HView x1, HVie
       void* w = avail ? ctx->ws + ((ctx->ws_top + 255) & ~(size_t)255) : nullptr;
       const int nterms = prec == OME_PREC_BF16X3 ? 2 : 3;
       if (gemm_kernel_choice(g) == 1) {
-        cudaError_t e = launch_gemm_packed(g, nterms, w, avail, ctx->num_sms, s);
+        void* pw = w;
+        size_t pavail = avail;
+        const size_t need = gemm_packed_bytes(g, nterms, ctx->num_sms);
+        if (need > avail) {
+          pw = overflow_scratch(ctx, need, s);
+          pavail = pw ? ctx->ovf_bytes : 0;
+        }
+        cudaError_t e = pw ? launch_gemm_packed(g, nterms, pw, pavail, ctx->num_sms, s) : cudaErrorNotSupported;
         if (e != cudaErrorNotSupported) {
           trace_path("  -> packed");
           return cuda_err(e, "packed bf16 split gemm");
@@ -712,6 +755,8 @@ int ome_ctx_create(int device, size_t workspace_bytes, ome_ctx** out) {
   c->ws = nullptr;
   c->ws_bytes = workspace_bytes;
   c->ws_top = 0;
+  c->ovf = nullptr;
+  c->ovf_bytes = 0;
   if (workspace_bytes) {
     cudaError_t e = cudaMalloc(&c->ws, workspace_bytes);
     if (e != cudaSuccess) {
@@ -726,6 +771,7 @@ int ome_ctx_create(int device, size_t workspace_bytes, ome_ctx** out) {
 int ome_ctx_destroy(ome_ctx* ctx) {
   if (!ctx) return OME_OK;
   if (ctx->ws) cudaFree(ctx->ws);
+  if (ctx->ovf) cudaFree(ctx->ovf);
   delete ctx;
   return OME_OK;
 }

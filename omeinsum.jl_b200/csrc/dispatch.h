@@ -11,6 +11,8 @@ struct ome_ctx {
   char* ws;          // device workspace (plan intermediates, scratch)
   size_t ws_bytes;
   size_t ws_top;     // bump pointer; reset by every top-level call
+  char* ovf;         // operand scratch of packed GEMMs that do not fit the workspace
+  size_t ovf_bytes;  // (grown on demand outside stream capture; freed with the context)
 };
 
 namespace ome {

@@ -292,8 +292,8 @@ int ome_plan_create(ome_ctx* ctx, ome_dtype dtype, int32_t ninputs, const int32_
   // FP32 binary nodes that the dispatcher sends to the packed-operand
   // tensor-core GEMM (M, N >= 256, K >= 512, >= 1 GFLOP) need their BF16
   // terms in the workspace: L * (M/128 + N/128 tiles) * K/32 k-steps * 24 KB,
-  // plus split partials and offset tables (at most 2 GB; a node that would
-  // need more runs the in-kernel-converter GEMM instead)
+  // plus split partials and offset tables (at most 2 GB here; a node that
+  // needs more takes its terms from the context's overflow scratch)
   auto packed_gemm_bytes = [&](int j, bool use_sliced) -> size_t {
     const PNode& n = p->nodes[j];
     if (dtype != OME_F32 || prec == OME_PREC_FP32 || n.args.size() != 2) return 0;

@@ -344,6 +344,58 @@ def einsum_(code: AbstractEinsum, xs: Sequence[Any], y, sx=True, sy=False, size_
     return y
 
 
+_COPY_STREAMS: Dict[int, Tuple[torch.cuda.Stream, torch.cuda.Stream]] = {}
+
+
+def einsum_many(jobs: Sequence[Tuple[AbstractEinsum, Sequence[Any], Dict[Any, int] | None]], window: int = 2):
+    """``[einsum(code, xs, size_dict) for code, xs, size_dict in jobs]`` for
+    independent contractions whose inputs live on the host, with the host link
+    kept busy in both directions: job i's inputs go up on one copy stream,
+    it runs on the current stream, and its result comes down on a second
+    copy stream while job i+1's inputs go up.  At most ``window`` jobs hold
+    device memory at once.  Results are page-locked host tensors (TropicalTensor
+    for tropical jobs), in job order; the call returns once all are on the
+    host.  Jobs whose inputs are already on the device run as ``einsum`` and
+    return device tensors."""
+    _require_b200()
+    jobs = list(jobs)
+    if window < 1:
+        raise ArgumentError("window must be at least 1")
+    dev = torch.device("cuda", torch.cuda.current_device())
+    if dev.index not in _COPY_STREAMS:
+        _COPY_STREAMS[dev.index] = (torch.cuda.Stream(dev), torch.cuda.Stream(dev))
+    up, down = _COPY_STREAMS[dev.index]
+    comp = torch.cuda.current_stream(dev)
+    outs: List[Any] = []
+    landed: List[Any] = [None] * len(jobs)
+    for i, (code, xs, size_dict) in enumerate(jobs):
+        xs = [_as_tensor(x) for x in xs]
+        raw = [x.data if isinstance(x, TropicalTensor) else x for x in xs]
+        if any(t.is_cuda for t in raw):
+            outs.append(einsum(code, xs, size_dict))
+            continue
+        if i >= window and landed[i - window] is not None:
+            landed[i - window].synchronize()
+        with torch.cuda.stream(up):
+            dx = [t.to(dev, non_blocking=True) for t in raw]
+        for t in dx:
+            t.record_stream(comp)
+        comp.wait_stream(up)
+        y = einsum(code, [TropicalTensor(t) if isinstance(x, TropicalTensor) else t for t, x in zip(dx, xs)],
+                   size_dict)
+        yt = y.data if isinstance(y, TropicalTensor) else y
+        down.wait_stream(comp)
+        with torch.cuda.stream(down):
+            h = torch.empty_strided(tuple(yt.shape), tuple(yt.stride()), dtype=yt.dtype, pin_memory=True)
+            h.copy_(yt, non_blocking=True)
+        yt.record_stream(down)
+        landed[i] = torch.cuda.Event()
+        landed[i].record(down)
+        outs.append(TropicalTensor(h) if isinstance(y, TropicalTensor) else h)
+    down.synchronize()
+    return outs
+
+
 def loop_einsum(code: EinCode, xs, size_dict=None):
     """``loop_einsum`` (src/loop_einsum.jl:8-12): the generic index kernel."""
     _require_b200()

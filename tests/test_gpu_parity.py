@@ -203,6 +203,35 @@ def test_large_gemm_packed(code, sizes):
     assert_match(got, oracle(ixs, iy, xs, sizes, "f32", wide=True), "f32", 1e-6)
 
 
+def test_packed_gemm_overflow_scratch():
+    """A GEMM whose BF16 operand terms (805 MB for M = N = 1024, K = 65536)
+    exceed the 256 MiB default workspace still runs on the packed kernel,
+    through the context's overflow scratch, and matches FP64."""
+    import ctypes as C
+    from omeinsum_b200 import _lib
+    _lib.release_workspaces()
+    torch.manual_seed(3)
+    a = torch.randn(1024, 65536, dtype=torch.float32, device="cuda")
+    b = torch.randn(65536, 1024, dtype=torch.float32, device="cuda")
+    A, B = a.t().contiguous().t(), b.t().contiguous().t()   # column-major
+    lib = _lib.load()
+    lib.ome_kernel_timing(8)
+    try:
+        y = ome.einsum(ome.EinCode([("i", "j"), ("j", "k")], ("i", "k")), [A, B])
+        torch.cuda.synchronize()
+        ome.device_status()
+        ms = (C.c_float * 8)()
+        names = (C.c_char_p * 8)()
+        cnt = C.c_int32()
+        lib.ome_kernel_times(8, ms, names, C.byref(cnt))
+    finally:
+        lib.ome_kernel_timing(0)
+    assert [names[i].decode() for i in range(cnt.value)] == ["k_gemm_packed"]
+    ref = A.double() @ B.double()
+    err = ((y.double() - ref).norm() / ref.norm()).item()
+    assert err < 1e-6, err
+
+
 @pytest.mark.parametrize("dt", ["f32", "f64", "c64", "i64", "trop", "bool"])
 @pytest.mark.parametrize("code,sizes", [
     ("bij,bjk->bik", dict(b=100, i=37, j=50, k=23)),     # ragged batch warp, partial 16x16 tiles
