@@ -160,62 +160,153 @@ static cudaError_t launch_gemm_simt_t(const GemmArgs& g, cudaStream_t s) {
 }
 
 // Batched GEMM whose batch mode is the contiguous one in A, B and C (Julia
-// column-major `bij,bjk->bik`: b fastest) with small M, N: lane = one of 32
-// consecutive batches, so every load and store of a warp is one contiguous
-// 128-byte row; warp w of 4 owns 4 rows of the block's 16 x 4 output tile
-// and keeps 4 x 4 accumulators (small tiles: enough warps in flight to hide
-// the L2 latency of the K loop, which is unrolled by 4; the fastest of the
-// tilings timed on b=512, 64^3); the 4 warps read the same B rows, which the
-// L1 serves after the first.  Plain algebra arithmetic in K order.
-template <class T> __device__ __forceinline__ T ld_ro(const T* p) { return *p; }
-template <> __device__ __forceinline__ float ld_ro<float>(const float* p) { return __ldg(p); }
-template <> __device__ __forceinline__ double ld_ro<double>(const double* p) { return __ldg(p); }
-
-// FULL: M % 16 == 0, N % 4 == 0 and L % 32 == 0 (no bounds tests in the loop)
-template <class A, bool FULL>
-__global__ void __launch_bounds__(128) k_gemm_bfast(const __grid_constant__ GemmArgs g) {
-  using T = typename A::T;
-  constexpr int TN = 4, RM = 4, WARPS = 4;
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int64_t b = (int64_t)blockIdx.x * 32 + lane;
-  if (!FULL && b >= g.L) return;
-  const int n0 = blockIdx.y * TN;
-  const int m0 = blockIdx.z * (RM * WARPS) + warp * RM;
-  // one mode per group, 32-bit strides inside a batch (checked by the host)
-  const int sma = (int)g.m_sa[0], smc = (int)g.m_sc[0], snb = (int)g.n_sb[0], snc = (int)g.n_sc[0];
-  const int ska = (int)g.k_sa[0], skb = (int)g.k_sb[0];
-  const int M = (int)g.M, N = (int)g.N, K = (int)g.K;
-  const T* __restrict__ ap = static_cast<const T*>(g.A) + mode_offset(b, g.nl, g.l_ext, g.l_sa) + (int64_t)m0 * sma;
-  const T* __restrict__ bp = static_cast<const T*>(g.B) + mode_offset(b, g.nl, g.l_ext, g.l_sb) + (int64_t)n0 * snb;
-  T* cp0 = static_cast<T*>(g.C) + mode_offset(b, g.nl, g.l_ext, g.l_sc) + (int64_t)m0 * smc + (int64_t)n0 * snc;
-  T acc[RM][TN];
+// column-major `bij,bjk->bik`: b fastest) with small M, N (<= 64).  A CTA of
+// 256 threads owns 4 consecutive batches and a 32-column slab of N; K runs in
+// chunks of 16 staged in shared memory (two buffers, the next chunk's global
+// loads in registers while the current one is multiplied).  Staging loads
+// walk the batch mode fastest (4 batches = 16 contiguous bytes for 4-byte
+// types), so each element of A and B leaves L2 once per slab instead of once
+// per register tile; each thread keeps 4 x 8 accumulators of one batch and
+// reads its operands from shared memory as broadcasts.  The tile leaves
+// through shared memory too, batch mode fastest.  Plain algebra arithmetic
+// in K order.
+// N consecutive elements from shared memory, 16 bytes per load when the
+// run is a whole number of 16-byte words (the caller keeps it aligned)
+template <class T, int N>
+__device__ __forceinline__ void lds_run(const T* p, T (&v)[N]) {
+  if constexpr ((sizeof(T) * N) % 16 == 0) {
+    constexpr int W = (int)(sizeof(T) * N / 16);
+    uint4 w[W];
+    const uint4* q = reinterpret_cast<const uint4*>(p);
 #pragma unroll
-  for (int r = 0; r < RM; ++r)
+    for (int i = 0; i < W; ++i) w[i] = q[i];
+    memcpy(v, w, sizeof(v));
+  } else {
 #pragma unroll
-    for (int c = 0; c < TN; ++c) acc[r][c] = A::zero();
-#pragma unroll 4
-  for (int k = 0; k < K; ++k) {
-    T av[RM], bv[TN];
-#pragma unroll
-    for (int r = 0; r < RM; ++r) av[r] = (FULL || m0 + r < M) ? ld_ro(ap + r * sma) : A::zero();
-#pragma unroll
-    for (int c = 0; c < TN; ++c) bv[c] = (FULL || n0 + c < N) ? ld_ro(bp + c * snb) : A::zero();
-#pragma unroll
-    for (int r = 0; r < RM; ++r)
-#pragma unroll
-      for (int c = 0; c < TN; ++c) acc[r][c] = A::add(acc[r][c], A::mul(av[r], bv[c]));
-    ap += ska;
-    bp += skb;
+    for (int i = 0; i < N; ++i) v[i] = p[i];
   }
+}
+
+namespace bs {
+constexpr int NB = 4, KC = 16, NS = 32, MT = 64, NT = 256;
+// every offset the compute reads (4*tm, 8*tn, the strides below) is a
+// multiple of 4 elements, so its runs are 16-byte aligned for 4-byte and
+// wider types
+constexpr int A_B = KC * MT + 8;   // elements per batch in an A stage (padded)
+constexpr int B_B = KC * NS + 8;   // elements per batch in a B stage
+constexpr int STAGE = NB * (A_B + B_B);
+constexpr int C_ROW = MT + 1;      // epilogue tile: [batch][n][m], padded rows
+constexpr int C_B = NS * C_ROW + 8;
+constexpr int ELEMS = 2 * STAGE > NB * C_B ? 2 * STAGE : NB * C_B;
+}  // namespace bs
+
+template <class A, bool FULL>
+__global__ void __launch_bounds__(bs::NT) k_gemm_bstage(const __grid_constant__ GemmArgs g) {
+  using namespace bs;
+  using T = typename A::T;
+  extern __shared__ __align__(16) unsigned char bs_raw[];
+  T* sm = reinterpret_cast<T*>(bs_raw);
+  const int t = threadIdx.x;
+  const int64_t b0 = (int64_t)blockIdx.x * NB;
+  const int n0 = blockIdx.y * NS;
+  const int M = (int)g.M, N = (int)g.N, K = (int)g.K;
+  const int sma = (int)g.m_sa[0], ska = (int)g.k_sa[0], snb = (int)g.n_sb[0], skb = (int)g.k_sb[0];
+  // staging roles: batch lb of the group; A row lm (all 16 k of a chunk);
+  // B column ln, k rows lk0 + 2q
+  const int lb = t & 3, lm = t >> 2, ln = (t >> 2) & 31, lk0 = t >> 7;
+  const bool bok = FULL || b0 + lb < g.L;
+  const T* ga = static_cast<const T*>(g.A);
+  const T* gb = static_cast<const T*>(g.B);
+  if (bok) {
+    ga += mode_offset(b0 + lb, g.nl, g.l_ext, g.l_sa) + (int64_t)lm * sma;
+    gb += mode_offset(b0 + lb, g.nl, g.l_ext, g.l_sb) + (int64_t)(n0 + ln) * snb + (int64_t)lk0 * skb;
+  }
+  const bool aok = bok && (FULL || lm < M), bnok = bok && (FULL || n0 + ln < N);
+  T ra[KC], rb[KC / 2];
+  auto load = [&](int k0) {
+#pragma unroll
+    for (int q = 0; q < KC; ++q)
+      ra[q] = aok && (FULL || k0 + q < K) ? ga[(int64_t)(k0 + q) * ska] : A::zero();
+#pragma unroll
+    for (int q = 0; q < KC / 2; ++q)
+      rb[q] = bnok && (FULL || k0 + lk0 + 2 * q < K) ? gb[(int64_t)(k0 + 2 * q) * skb] : A::zero();
+  };
+  auto store = [&](int st) {
+    T* as = sm + st * STAGE + lb * A_B + lm;
+    T* bsm = sm + st * STAGE + NB * A_B + lb * B_B + lk0 * NS + ln;
+#pragma unroll
+    for (int q = 0; q < KC; ++q) as[q * MT] = ra[q];
+#pragma unroll
+    for (int q = 0; q < KC / 2; ++q) bsm[2 * q * NS] = rb[q];
+  };
+  // 16-byte types (complex128) stage straight from global memory after the
+  // multiply: 4 x 8 accumulators leave no registers for a prefetch
+  constexpr bool PREF = sizeof(T) < 16;
+  auto load_store = [&](int k0, int st) {
+    T* as = sm + st * STAGE + lb * A_B + lm;
+    T* bsm = sm + st * STAGE + NB * A_B + lb * B_B + lk0 * NS + ln;
+#pragma unroll 4
+    for (int q = 0; q < KC; ++q)
+      as[q * MT] = aok && (FULL || k0 + q < K) ? ga[(int64_t)(k0 + q) * ska] : A::zero();
+#pragma unroll 4
+    for (int q = 0; q < KC / 2; ++q)
+      bsm[2 * q * NS] = bnok && (FULL || k0 + lk0 + 2 * q < K) ? gb[(int64_t)(k0 + 2 * q) * skb] : A::zero();
+  };
+  // compute roles: batch cb, rows 4*tm.., columns 8*tn..
+  const int cb = t >> 6, tm = (t >> 2) & 15, tn = t & 3;
+  T acc[4][8];
+#pragma unroll
+  for (int r = 0; r < 4; ++r)
+#pragma unroll
+    for (int c = 0; c < 8; ++c) acc[r][c] = A::zero();
+  const int nchunks = (K + KC - 1) / KC;
+  if (PREF) {
+    load(0);
+    store(0);
+  } else {
+    load_store(0, 0);
+  }
+  __syncthreads();
+  for (int ch = 0; ch < nchunks; ++ch) {
+    const int st = ch & 1;
+    if (PREF && ch + 1 < nchunks) load((ch + 1) * KC);
+    const T* as = sm + st * STAGE + cb * A_B + 4 * tm;
+    const T* bsm = sm + st * STAGE + NB * A_B + cb * B_B + 8 * tn;
+#pragma unroll 4
+    for (int kk = 0; kk < KC; ++kk) {
+      T av[4], bv[8];
+      lds_run(as + kk * MT, av);
+      lds_run(bsm + kk * NS, bv);
+#pragma unroll
+      for (int r = 0; r < 4; ++r)
+#pragma unroll
+        for (int c = 0; c < 8; ++c) acc[r][c] = A::add(acc[r][c], A::mul(av[r], bv[c]));
+    }
+    if (ch + 1 < nchunks) {
+      if (PREF) store(st ^ 1);
+      else load_store((ch + 1) * KC, st ^ 1);
+    }
+    __syncthreads();
+  }
+  // tile -> shared [batch][n][m] -> C with the batch mode fastest
+  {
+    T* cs = sm + cb * C_B + (8 * tn) * C_ROW + 4 * tm;
+#pragma unroll
+    for (int c = 0; c < 8; ++c)
+#pragma unroll
+      for (int r = 0; r < 4; ++r) cs[c * C_ROW + r] = acc[r][c];
+  }
+  __syncthreads();
+  if (!bok || !(FULL || lm < M)) return;
   const T sx = scalar_as<T>(g.sx), sy = scalar_as<T>(g.sy);
-#pragma unroll
-  for (int r = 0; r < RM; ++r)
-#pragma unroll
-    for (int c = 0; c < TN; ++c)
-      if (FULL || (m0 + r < M && n0 + c < N)) {
-        T* cp = cp0 + r * smc + c * snc;
-        *cp = epilogue<A>(acc[r][c], cp, sx, sy, g.sy_zero, g.sx_one);
-      }
+  T* cp = static_cast<T*>(g.C) + mode_offset(b0 + lb, g.nl, g.l_ext, g.l_sc) + (int64_t)lm * g.m_sc[0] +
+          (int64_t)n0 * g.n_sc[0];
+  const T* cs = sm + lb * C_B + lm;
+  const int nn = FULL ? NS : min(NS, N - n0);
+  for (int q = 0; q < nn; ++q) {
+    T* yp = cp + (int64_t)q * g.n_sc[0];
+    *yp = epilogue<A>(cs[q * C_ROW], yp, sx, sy, g.sy_zero, g.sx_one);
+  }
 }
 
 bool gemm_bfast_applies(const GemmArgs& g) {
@@ -226,19 +317,31 @@ bool gemm_bfast_applies(const GemmArgs& g) {
          small(g.K, g.k_sa[0]) && small(g.K, g.k_sb[0]);
 }
 
+template <class A>
+static cudaError_t launch_gemm_bstage_t(const GemmArgs& g, cudaStream_t s) {
+  const size_t smem = (size_t)bs::ELEMS * sizeof(typename A::T);
+  static bool attr = false;
+  if (!attr) {
+    cudaError_t e = cudaFuncSetAttribute(k_gemm_bstage<A, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e == cudaSuccess)
+      e = cudaFuncSetAttribute(k_gemm_bstage<A, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    attr = true;
+  }
+  const dim3 grid((unsigned)((g.L + bs::NB - 1) / bs::NB), (unsigned)((g.N + bs::NS - 1) / bs::NS));
+  const bool full = g.M == bs::MT && g.N % bs::NS == 0 && g.K % bs::KC == 0 && g.L % bs::NB == 0;
+  if (full) k_gemm_bstage<A, true><<<grid, bs::NT, smem, s>>>(g);
+  else k_gemm_bstage<A, false><<<grid, bs::NT, smem, s>>>(g);
+  count_launch();
+  return cudaGetLastError();
+}
+
 cudaError_t launch_gemm_bfast(ome_dtype dt, const GemmArgs& g, cudaStream_t s) {
   if (g.M == 0 || g.N == 0 || g.L == 0) return cudaSuccess;
   if (!gemm_bfast_applies(g)) return cudaErrorNotSupported;
-  const dim3 grid((unsigned)((g.L + 31) / 32), (unsigned)((g.N + 3) / 4), (unsigned)((g.M + 15) / 16));
   cudaError_t e = cudaErrorInvalidValue;
-  const bool full = g.M % 16 == 0 && g.N % 4 == 0 && g.L % 32 == 0;
-  KernelTimer kt(s, "k_gemm_bfast");
-  OME_DISPATCH(dt, ALG, {
-    if (full) k_gemm_bfast<ALG, true><<<grid, 128, 0, s>>>(g);
-    else k_gemm_bfast<ALG, false><<<grid, 128, 0, s>>>(g);
-    count_launch();
-    e = cudaGetLastError();
-  });
+  KernelTimer kt(s, "k_gemm_bstage");
+  OME_DISPATCH(dt, ALG, e = launch_gemm_bstage_t<ALG>(g, s));
   return e;
 }
 

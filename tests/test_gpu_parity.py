@@ -237,6 +237,8 @@ def test_packed_gemm_overflow_scratch():
     ("bij,bjk->bik", dict(b=100, i=37, j=50, k=23)),     # ragged batch warp, partial 16x16 tiles
     ("bij,bkj->bki", dict(b=64, i=64, j=9, k=64)),        # transposed operands, full tiles
     ("bcij,bcjk->bcik", dict(b=40, c=3, i=5, j=7, k=6)),  # two batch modes, b innermost
+    ("bij,bjk->bik", dict(b=101, i=64, j=200, k=40)),    # ragged batch group, 13 K chunks, partial second N slab
+    ("bij,bjk->bik", dict(b=64, i=64, j=32, k=64)),      # no bounds tests (M = 64, N, K, L whole)
 ])
 def test_batch_innermost_gemm(code, sizes, dt):
     """Batches of small GEMMs whose batch mode is contiguous in every tensor
