@@ -370,7 +370,7 @@ def serve_section(ome, dev, njobs=32, rate=2000.0, seed=10, nmin=40, nmax=200, g
     st.update({"workload": f"{njobs} jobs, Poisson {rate:.0f}/s (seed {seed}), n uniform even [{nmin},{nmax}], "
                            "bond 2, unscaled FP32 normal(0,1), 10% gradient jobs, greedy order (best of 10) + greedy "
                            "slicing to 2^27 (client side), 16 slots sharing a 150 GB workspace budget",
-               "submitted": njobs, "incomplete": njobs - len(done), "cap_s": cap_s,
+               "submitted": njobs, "incomplete": njobs - len(done) - int(st.get("rejected", 0)), "cap_s": cap_s,
                "client_planning_s": plan_s, "n_of_completed": sorted(int(len(j.xs)) for j in done)})
     return st
 

@@ -161,17 +161,15 @@ static cudaError_t launch_gemm_simt_t(const GemmArgs& g, cudaStream_t s) {
 
 // Batched GEMM whose batch mode is the contiguous one in A, B and C (Julia
 // column-major `bij,bjk->bik`: b fastest) with small M, N (<= 64).  A CTA of
-// 256 threads owns 4 consecutive batches and a 32-column slab of N; K runs in
-// chunks of 16 staged in shared memory (two buffers, the next chunk's global
-// loads in registers while the current one is multiplied).  Staging loads
-// walk the batch mode fastest (4 batches = 16 contiguous bytes for 4-byte
-// types), so each element of A and B leaves L2 once per slab instead of once
-// per register tile; each thread keeps 4 x 8 accumulators of one batch and
-// reads its operands from shared memory as broadcasts.  The tile leaves
-// through shared memory too, batch mode fastest.  Plain algebra arithmetic
-// in K order.
-// N consecutive elements from shared memory, 16 bytes per load when the
-// run is a whole number of 16-byte words (the caller keeps it aligned)
+// 256 threads owns 4 consecutive batches and an NS-column slab of N (64:
+// all of it, for 4-byte types with N > 32; otherwise 32); K runs in chunks of 16 staged in shared memory
+// (two buffers, the next chunk's global loads in registers while the current
+// one is multiplied).  Staging loads walk the batch mode fastest (4 batches =
+// 16 contiguous bytes for 4-byte types), so each element of A and B leaves
+// L2 once per slab instead of once per register tile; each thread keeps
+// 8 x NS/8 accumulators of one batch and reads its operands from shared
+// memory as 16-byte broadcasts (B in runs of 4 columns, conflict-free).  The tile leaves through shared memory too,
+// batch mode fastest.  Plain algebra arithmetic in K order.
 template <class T, int N>
 __device__ __forceinline__ void lds_run(const T* p, T (&v)[N]) {
   if constexpr ((sizeof(T) * N) % 16 == 0) {
@@ -187,22 +185,27 @@ __device__ __forceinline__ void lds_run(const T* p, T (&v)[N]) {
   }
 }
 
-namespace bs {
-constexpr int NB = 4, KC = 16, NS = 32, MT = 64, NT = 256;
-// every offset the compute reads (4*tm, 8*tn, the strides below) is a
-// multiple of 4 elements, so its runs are 16-byte aligned for 4-byte and
-// wider types
-constexpr int A_B = KC * MT + 8;   // elements per batch in an A stage (padded)
-constexpr int B_B = KC * NS + 8;   // elements per batch in a B stage
-constexpr int STAGE = NB * (A_B + B_B);
-constexpr int C_ROW = MT + 1;      // epilogue tile: [batch][n][m], padded rows
-constexpr int C_B = NS * C_ROW + 8;
-constexpr int ELEMS = 2 * STAGE > NB * C_B ? 2 * STAGE : NB * C_B;
-}  // namespace bs
+template <int NS_> struct BsCfg {
+  static constexpr int NB = 4, KC = 16, NS = NS_, MT = 64, NT = 256;
+  static constexpr int TR = 8, TC = NS / 8;          // thread tile: rows x columns
+  static constexpr int KSTEP = 64 / NS;              // B staging: k rows lk0, lk0 + KSTEP, ...
+  // every offset the compute reads (8*tm, 4*tn, 32, the strides below) is a
+  // multiple of 4 elements, so its runs are 16-byte aligned for 4-byte and
+  // wider types
+  static constexpr int A_B = KC * MT + 8;            // elements per batch in an A stage (padded)
+  static constexpr int B_B = KC * NS + 8;            // elements per batch in a B stage
+  static constexpr int STAGE = NB * (A_B + B_B);
+  static constexpr int C_ROW = MT + 1;               // epilogue tile: [batch][n][m], padded rows
+  static constexpr int C_B = NS * C_ROW + 8;
+  static constexpr int ELEMS = 2 * STAGE > NB * C_B ? 2 * STAGE : NB * C_B;
+};
 
-template <class A, bool FULL>
-__global__ void __launch_bounds__(bs::NT) k_gemm_bstage(const __grid_constant__ GemmArgs g) {
-  using namespace bs;
+template <class A, bool FULL, int NS_>
+__global__ void __launch_bounds__(256, 1) k_gemm_bstage(const __grid_constant__ GemmArgs g) {
+  using Cf = BsCfg<NS_>;
+  constexpr int NB = Cf::NB, KC = Cf::KC, NS = Cf::NS, MT = Cf::MT, TR = Cf::TR, TC = Cf::TC;
+  constexpr int KSTEP = Cf::KSTEP, A_B = Cf::A_B, B_B = Cf::B_B, STAGE = Cf::STAGE, C_ROW = Cf::C_ROW,
+                C_B = Cf::C_B;
   using T = typename A::T;
   extern __shared__ __align__(16) unsigned char bs_raw[];
   T* sm = reinterpret_cast<T*>(bs_raw);
@@ -212,8 +215,8 @@ __global__ void __launch_bounds__(bs::NT) k_gemm_bstage(const __grid_constant__ 
   const int M = (int)g.M, N = (int)g.N, K = (int)g.K;
   const int sma = (int)g.m_sa[0], ska = (int)g.k_sa[0], snb = (int)g.n_sb[0], skb = (int)g.k_sb[0];
   // staging roles: batch lb of the group; A row lm (all 16 k of a chunk);
-  // B column ln, k rows lk0 + 2q
-  const int lb = t & 3, lm = t >> 2, ln = (t >> 2) & 31, lk0 = t >> 7;
+  // B column ln, k rows lk0 + KSTEP*q
+  const int lb = t & 3, lm = t >> 2, ln = (t >> 2) % NS, lk0 = (t >> 2) / NS;
   const bool bok = FULL || b0 + lb < g.L;
   const T* ga = static_cast<const T*>(g.A);
   const T* gb = static_cast<const T*>(g.B);
@@ -222,14 +225,14 @@ __global__ void __launch_bounds__(bs::NT) k_gemm_bstage(const __grid_constant__ 
     gb += mode_offset(b0 + lb, g.nl, g.l_ext, g.l_sb) + (int64_t)(n0 + ln) * snb + (int64_t)lk0 * skb;
   }
   const bool aok = bok && (FULL || lm < M), bnok = bok && (FULL || n0 + ln < N);
-  T ra[KC], rb[KC / 2];
+  T ra[KC], rb[KC / KSTEP];
   auto load = [&](int k0) {
 #pragma unroll
     for (int q = 0; q < KC; ++q)
       ra[q] = aok && (FULL || k0 + q < K) ? ga[(int64_t)(k0 + q) * ska] : A::zero();
 #pragma unroll
-    for (int q = 0; q < KC / 2; ++q)
-      rb[q] = bnok && (FULL || k0 + lk0 + 2 * q < K) ? gb[(int64_t)(k0 + 2 * q) * skb] : A::zero();
+    for (int q = 0; q < KC / KSTEP; ++q)
+      rb[q] = bnok && (FULL || k0 + lk0 + KSTEP * q < K) ? gb[(int64_t)(k0 + KSTEP * q) * skb] : A::zero();
   };
   auto store = [&](int st) {
     T* as = sm + st * STAGE + lb * A_B + lm;
@@ -237,10 +240,10 @@ __global__ void __launch_bounds__(bs::NT) k_gemm_bstage(const __grid_constant__ 
 #pragma unroll
     for (int q = 0; q < KC; ++q) as[q * MT] = ra[q];
 #pragma unroll
-    for (int q = 0; q < KC / 2; ++q) bsm[2 * q * NS] = rb[q];
+    for (int q = 0; q < KC / KSTEP; ++q) bsm[KSTEP * q * NS] = rb[q];
   };
   // 16-byte types (complex128) stage straight from global memory after the
-  // multiply: 4 x 8 accumulators leave no registers for a prefetch
+  // multiply: the accumulators leave no registers for a prefetch
   constexpr bool PREF = sizeof(T) < 16;
   auto load_store = [&](int k0, int st) {
     T* as = sm + st * STAGE + lb * A_B + lm;
@@ -249,16 +252,19 @@ __global__ void __launch_bounds__(bs::NT) k_gemm_bstage(const __grid_constant__ 
     for (int q = 0; q < KC; ++q)
       as[q * MT] = aok && (FULL || k0 + q < K) ? ga[(int64_t)(k0 + q) * ska] : A::zero();
 #pragma unroll 4
-    for (int q = 0; q < KC / 2; ++q)
-      bsm[2 * q * NS] = bnok && (FULL || k0 + lk0 + 2 * q < K) ? gb[(int64_t)(k0 + 2 * q) * skb] : A::zero();
+    for (int q = 0; q < KC / KSTEP; ++q)
+      bsm[KSTEP * q * NS] =
+          bnok && (FULL || k0 + lk0 + KSTEP * q < K) ? gb[(int64_t)(k0 + KSTEP * q) * skb] : A::zero();
   };
-  // compute roles: batch cb, rows 4*tm.., columns 8*tn..
-  const int cb = t >> 6, tm = (t >> 2) & 15, tn = t & 3;
-  T acc[4][8];
+  // compute roles: batch cb, rows TR*tm.., columns 4*tn.. (and 32 + 4*tn..
+  // for 8-column tiles: a warp's 16-byte reads of B stay in one 128-byte row
+  // of banks)
+  const int cb = t >> 6, tm = (t >> 3) & 7, tn = t & 7;
+  T acc[TR][TC];
 #pragma unroll
-  for (int r = 0; r < 4; ++r)
+  for (int r = 0; r < TR; ++r)
 #pragma unroll
-    for (int c = 0; c < 8; ++c) acc[r][c] = A::zero();
+    for (int c = 0; c < TC; ++c) acc[r][c] = A::zero();
   const int nchunks = (K + KC - 1) / KC;
   if (PREF) {
     load(0);
@@ -270,17 +276,23 @@ __global__ void __launch_bounds__(bs::NT) k_gemm_bstage(const __grid_constant__ 
   for (int ch = 0; ch < nchunks; ++ch) {
     const int st = ch & 1;
     if (PREF && ch + 1 < nchunks) load((ch + 1) * KC);
-    const T* as = sm + st * STAGE + cb * A_B + 4 * tm;
-    const T* bsm = sm + st * STAGE + NB * A_B + cb * B_B + 8 * tn;
-#pragma unroll 4
+    const T* as = sm + st * STAGE + cb * A_B + TR * tm;
+    const T* bsm = sm + st * STAGE + NB * A_B + cb * B_B + 4 * tn;
+#pragma unroll 2
     for (int kk = 0; kk < KC; ++kk) {
-      T av[4], bv[8];
+      T av[TR], bv[TC];
       lds_run(as + kk * MT, av);
-      lds_run(bsm + kk * NS, bv);
 #pragma unroll
-      for (int r = 0; r < 4; ++r)
+      for (int h = 0; h < TC / 4; ++h) {
+        T b4[4];
+        lds_run(bsm + kk * NS + 32 * h, b4);
 #pragma unroll
-        for (int c = 0; c < 8; ++c) acc[r][c] = A::add(acc[r][c], A::mul(av[r], bv[c]));
+        for (int c = 0; c < 4; ++c) bv[4 * h + c] = b4[c];
+      }
+#pragma unroll
+      for (int r = 0; r < TR; ++r)
+#pragma unroll
+        for (int c = 0; c < TC; ++c) acc[r][c] = A::add(acc[r][c], A::mul(av[r], bv[c]));
     }
     if (ch + 1 < nchunks) {
       if (PREF) store(st ^ 1);
@@ -290,11 +302,11 @@ __global__ void __launch_bounds__(bs::NT) k_gemm_bstage(const __grid_constant__ 
   }
   // tile -> shared [batch][n][m] -> C with the batch mode fastest
   {
-    T* cs = sm + cb * C_B + (8 * tn) * C_ROW + 4 * tm;
+    T* cs = sm + cb * C_B + (4 * tn) * C_ROW + TR * tm;
 #pragma unroll
-    for (int c = 0; c < 8; ++c)
+    for (int c = 0; c < TC; ++c)
 #pragma unroll
-      for (int r = 0; r < 4; ++r) cs[c * C_ROW + r] = acc[r][c];
+      for (int r = 0; r < TR; ++r) cs[((c >> 2) * 32 + (c & 3)) * C_ROW + r] = acc[r][c];
   }
   __syncthreads();
   if (!bok || !(FULL || lm < M)) return;
@@ -317,23 +329,35 @@ bool gemm_bfast_applies(const GemmArgs& g) {
          small(g.K, g.k_sa[0]) && small(g.K, g.k_sb[0]);
 }
 
-template <class A>
+template <class A, int NS>
 static cudaError_t launch_gemm_bstage_t(const GemmArgs& g, cudaStream_t s) {
-  const size_t smem = (size_t)bs::ELEMS * sizeof(typename A::T);
+  using Cf = BsCfg<NS>;
+  const size_t smem = (size_t)Cf::ELEMS * sizeof(typename A::T);
   static bool attr = false;
   if (!attr) {
-    cudaError_t e = cudaFuncSetAttribute(k_gemm_bstage<A, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaError_t e =
+        cudaFuncSetAttribute(k_gemm_bstage<A, true, NS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e == cudaSuccess)
-      e = cudaFuncSetAttribute(k_gemm_bstage<A, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      e = cudaFuncSetAttribute(k_gemm_bstage<A, false, NS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     attr = true;
   }
-  const dim3 grid((unsigned)((g.L + bs::NB - 1) / bs::NB), (unsigned)((g.N + bs::NS - 1) / bs::NS));
-  const bool full = g.M == bs::MT && g.N % bs::NS == 0 && g.K % bs::KC == 0 && g.L % bs::NB == 0;
-  if (full) k_gemm_bstage<A, true><<<grid, bs::NT, smem, s>>>(g);
-  else k_gemm_bstage<A, false><<<grid, bs::NT, smem, s>>>(g);
+  const dim3 grid((unsigned)((g.L + Cf::NB - 1) / Cf::NB), (unsigned)((g.N + NS - 1) / NS));
+  const bool full = g.M == Cf::MT && g.N % NS == 0 && g.K % Cf::KC == 0 && g.L % Cf::NB == 0;
+  if (full) k_gemm_bstage<A, true, NS><<<grid, Cf::NT, smem, s>>>(g);
+  else k_gemm_bstage<A, false, NS><<<grid, Cf::NT, smem, s>>>(g);
   count_launch();
   return cudaGetLastError();
+}
+
+// 64-column slabs (8 x 8 thread tiles) for types of at most 4 bytes; wider
+// types keep 8 x 4 tiles, whose accumulators already fill the registers
+template <class A>
+static cudaError_t launch_gemm_bstage(const GemmArgs& g, cudaStream_t s) {
+  if constexpr (sizeof(typename A::T) <= 4) {
+    if (g.N > 32) return launch_gemm_bstage_t<A, 64>(g, s);
+  }
+  return launch_gemm_bstage_t<A, 32>(g, s);
 }
 
 cudaError_t launch_gemm_bfast(ome_dtype dt, const GemmArgs& g, cudaStream_t s) {
@@ -341,7 +365,7 @@ cudaError_t launch_gemm_bfast(ome_dtype dt, const GemmArgs& g, cudaStream_t s) {
   if (!gemm_bfast_applies(g)) return cudaErrorNotSupported;
   cudaError_t e = cudaErrorInvalidValue;
   KernelTimer kt(s, "k_gemm_bstage");
-  OME_DISPATCH(dt, ALG, e = launch_gemm_bstage_t<ALG>(g, s));
+  OME_DISPATCH(dt, ALG, e = launch_gemm_bstage<ALG>(g, s));
   return e;
 }
 
