@@ -594,10 +594,9 @@ static int run_binary(ome_ctx* ctx, cudaStream_t s, ome_dtype dt, HView x1, HVie
     }
     if (dt == OME_F32 && prec != OME_PREC_FP32 && gemm_split_supported(g)) {
       // output mode groups of several modes: C offset tables for the epilogues
-      if (g.nm > 1 || g.nn > 1) {
-        int64_t* tab = static_cast<int64_t*>(ws_alloc(ctx, (size_t)(M + N) * sizeof(int64_t)));
-        if (tab) OME_CK(cuda_err(launch_c_offsets(g, tab, s), "offset tables"));
-      }
+      // (filled by the packed GEMM's pack launch, else by their own kernel)
+      int64_t* tab = nullptr;
+      if (g.nm > 1 || g.nn > 1) tab = static_cast<int64_t*>(ws_alloc(ctx, (size_t)(M + N) * sizeof(int64_t)));
       size_t avail = ctx->ws_bytes > ctx->ws_top ? ctx->ws_bytes - ((ctx->ws_top + 255) & ~(size_t)255) : 0;
       void* w = avail ? ctx->ws + ((ctx->ws_top + 255) & ~(size_t)255) : nullptr;
       const int nterms = prec == OME_PREC_BF16X3 ? 2 : 3;
@@ -609,13 +608,14 @@ static int run_binary(ome_ctx* ctx, cudaStream_t s, ome_dtype dt, HView x1, HVie
           pw = overflow_scratch(ctx, need, s);
           pavail = pw ? ctx->ovf_bytes : 0;
         }
-        cudaError_t e = pw ? launch_gemm_packed(g, nterms, pw, pavail, ctx->num_sms, s) : cudaErrorNotSupported;
+        cudaError_t e = pw ? launch_gemm_packed(g, nterms, pw, pavail, ctx->num_sms, s, tab) : cudaErrorNotSupported;
         if (e != cudaErrorNotSupported) {
           trace_path("  -> packed");
           return cuda_err(e, "packed bf16 split gemm");
         }
         cudaGetLastError();
       }
+      if (tab) OME_CK(cuda_err(launch_c_offsets(g, tab, s), "offset tables"));
       trace_path("  -> tc");
       cudaError_t e = launch_gemm_split(g, nterms, w, avail, ctx->num_sms, s);
       if (e != cudaErrorNotSupported) return cuda_err(e, "bf16 split gemm");

@@ -30,6 +30,7 @@
 //    kernel records g_ome_timeout, stops waiting and frees its TMEM.
 #include <cuda_bf16.h>
 #include <string.h>
+#include <utility>
 #include "kernels.h"
 
 namespace ome {
@@ -584,10 +585,21 @@ template <int NT> struct Cfg {
 struct PackArgs {
   const float* X;
   unsigned char* P;   // [L][RT][NKT] blobs of NT x 8 KB
+  int64_t* c_tab;     // C offset of every row (NULL: no table), from c_str
   int64_t R, K, L, RT, NKT;
   int nr, nk, nl, kfast;
-  int64_t r_ext[MAXG], r_str[MAXG], k_ext[MAXG], k_str[MAXG], l_ext[MAXG], l_str[MAXG];
+  int64_t r_ext[MAXG], r_str[MAXG], k_ext[MAXG], k_str[MAXG], l_ext[MAXG], l_str[MAXG], c_str[MAXG];
 };
+
+// Programmatic dependent launch: a kernel launched with the programmatic
+// stream-serialisation attribute may start while the previous kernel in its
+// stream finishes; it runs its set-up, then waits here until that kernel has
+// completed and its writes are visible.  The previous kernel lets it start
+// once all its own blocks are running.
+__device__ __forceinline__ void griddep_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void griddep_launch_dependents() {
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
 
 struct PkArgs {
   GemmArgs g;                  // C, M, N, L and the epilogue
@@ -599,38 +611,59 @@ struct PkArgs {
 };
 
 template <int NT>
-__global__ void __launch_bounds__(256) k_pack_split(const __grid_constant__ PackArgs p) {
+__device__ __forceinline__ void pack_blob(const PackArgs& p, int64_t b, int warp, int lane) {
   using namespace pk;
+  const int64_t kt = b % p.NKT;
+  const int64_t r2 = b / p.NKT;
+  const int64_t rt = r2 % p.RT;
+  const int64_t l = r2 / p.RT;
+  const int64_t loff = mode_offset(l, p.nl, p.l_ext, p.l_str);
+  uint4* out = reinterpret_cast<uint4*>(p.P + b * (int64_t)(NT * TILE_BYTES));
+  float v[2][8];
+  int so[2];
+#pragma unroll
+  for (int j = 0; j < 2; ++j) {
+    // the converter mapping of k_gemm_bf16x3 over 16 virtual warps: each
+    // quarter-warp writes one contiguous 128-byte core matrix
+    const int vw = warp + 8 * j;
+    int row, kc;
+    if (p.kfast) { row = 8 * vw + (lane & 7); kc = lane >> 3; }
+    else { row = 32 * (vw & 3) + lane; kc = vw >> 2; }
+    const int64_t r = rt * BM + row;
+    const int64_t roff = r < p.R ? loff + goff(r, p.nr, p.r_ext, p.r_str) : -1;
+    load_unit(p.X, roff, kt * BK + kc * 8, p.K, p.kfast, p.nk, p.k_ext, p.k_str, v[j]);
+    so[j] = ((row >> 3) * 4 + kc) * 8 + (row & 7);
+  }
+#pragma unroll
+  for (int j = 0; j < 2; ++j) {
+    uint4 t[NT];
+    split8<NT>(v[j], t);
+#pragma unroll
+    for (int u = 0; u < NT; ++u) out[u * (TILE_BYTES / 16) + so[j]] = t[u];
+  }
+}
+
+// One launch packs A, then B, then fills the C offset tables of the rows of
+// A (M) and B (N) when they are asked for: work unit = one blob or 256
+// table entries, grid-stride over all of them.
+template <int NT>
+__global__ void __launch_bounds__(256) k_pack_split(const __grid_constant__ PackArgs pa,
+                                                    const __grid_constant__ PackArgs pb) {
+  griddep_launch_dependents();
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int64_t nblobs = p.L * p.RT * p.NKT;
-  for (int64_t b = blockIdx.x; b < nblobs; b += gridDim.x) {
-    const int64_t kt = b % p.NKT;
-    const int64_t r2 = b / p.NKT;
-    const int64_t rt = r2 % p.RT;
-    const int64_t l = r2 / p.RT;
-    const int64_t loff = mode_offset(l, p.nl, p.l_ext, p.l_str);
-    uint4* out = reinterpret_cast<uint4*>(p.P + b * (int64_t)(NT * TILE_BYTES));
-    float v[2][8];
-    int so[2];
-#pragma unroll
-    for (int j = 0; j < 2; ++j) {
-      // the converter mapping of k_gemm_bf16x3 over 16 virtual warps: each
-      // quarter-warp writes one contiguous 128-byte core matrix
-      const int vw = warp + 8 * j;
-      int row, kc;
-      if (p.kfast) { row = 8 * vw + (lane & 7); kc = lane >> 3; }
-      else { row = 32 * (vw & 3) + lane; kc = vw >> 2; }
-      const int64_t r = rt * BM + row;
-      const int64_t roff = r < p.R ? loff + goff(r, p.nr, p.r_ext, p.r_str) : -1;
-      load_unit(p.X, roff, kt * BK + kc * 8, p.K, p.kfast, p.nk, p.k_ext, p.k_str, v[j]);
-      so[j] = ((row >> 3) * 4 + kc) * 8 + (row & 7);
-    }
-#pragma unroll
-    for (int j = 0; j < 2; ++j) {
-      uint4 t[NT];
-      split8<NT>(v[j], t);
-#pragma unroll
-      for (int u = 0; u < NT; ++u) out[u * (TILE_BYTES / 16) + so[j]] = t[u];
+  const int64_t na = pa.L * pa.RT * pa.NKT, nb = pb.L * pb.RT * pb.NKT;
+  const int64_t ta = pa.c_tab ? (pa.R + 255) / 256 : 0, tb = pb.c_tab ? (pb.R + 255) / 256 : 0;
+  const int64_t total = na + nb + ta + tb;
+  for (int64_t u = blockIdx.x; u < total; u += gridDim.x) {
+    if (u < na) {
+      pack_blob<NT>(pa, u, warp, lane);
+    } else if (u < na + nb) {
+      pack_blob<NT>(pb, u - na, warp, lane);
+    } else {
+      const bool first = u < na + nb + ta;
+      const PackArgs& p = first ? pa : pb;
+      const int64_t i = (u - na - nb - (first ? 0 : ta)) * 256 + threadIdx.x;
+      if (i < p.R) p.c_tab[i] = mode_offset(i, p.nr, p.r_ext, p.c_str);
     }
   }
 }
@@ -693,6 +726,9 @@ __global__ void __launch_bounds__(pk::NTHREADS, 1) k_gemm_packed(const __grid_co
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
+  // the packs (and the offset tables) are complete from here on
+  griddep_wait();
+  griddep_launch_dependents();
   const uint32_t tmem = *tmem_slot;
   auto tmem_main = [&](int b) { return tmem + (uint32_t)(256 * b); };
   auto tmem_cross = [&](int b) { return tmem + (uint32_t)(256 * b + 128); };
@@ -860,6 +896,7 @@ __global__ void __launch_bounds__(pk::NTHREADS, 1) k_gemm_packed(const __grid_co
 // Sum the S split partials of each split tile in split order; αβ epilogue.
 __global__ void __launch_bounds__(256) k_splitk_tiles(const __grid_constant__ PkArgs t) {
   using namespace pk;
+  griddep_wait();
   const GemmArgs& g = t.g;
   const float sx = scalar_as<float>(g.sx), sy = scalar_as<float>(g.sy);
   float* Cp = static_cast<float*>(g.C);
@@ -911,8 +948,25 @@ size_t gemm_packed_bytes(const GemmArgs& g, int nterms, int num_sms) {
   return (size_t)g.L * (TM + TN) * NKT * blob + (size_t)num_sms * BM * BN * 4 + 1024;
 }
 
+// Launch with programmatic stream serialisation (see griddep_wait).
+template <class... KArgs, class... Args>
+static cudaError_t launch_pdl(void (*kernel)(KArgs...), unsigned grid, unsigned block, size_t smem, cudaStream_t s,
+                              Args&&... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(grid);
+  cfg.blockDim = dim3(block);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
+}
+
 cudaError_t launch_gemm_packed(const GemmArgs& g, int nterms, void* workspace, size_t ws_bytes, int num_sms,
-                               cudaStream_t s) {
+                               cudaStream_t s, int64_t* ctab) {
   using namespace pk;
   if (!gemm_split_supported(g) || (nterms != 2 && nterms != 3)) return cudaErrorNotSupported;
   static bool attr_set[2] = {false, false};
@@ -954,23 +1008,27 @@ cudaError_t launch_gemm_packed(const GemmArgs& g, int nterms, void* workspace, s
   PackArgs pa, pb;
   pack_args(pa, static_cast<const float*>(g.A), PA, g.M, g.nm, g.m_ext, g.m_sa, g, g.k_sa, g.l_sa);
   pack_args(pb, static_cast<const float*>(g.B), PB, g.N, g.nn, g.n_ext, g.n_sb, g, g.k_sb, g.l_sb);
-  const int64_t grid_cap = (int64_t)num_sms * 8;
-  const unsigned ga = (unsigned)std::min<int64_t>(g.L * TM * NKT, grid_cap);
-  const unsigned gb = (unsigned)std::min<int64_t>(g.L * TN * NKT, grid_cap);
-  if (nterms == 2) {
-    k_pack_split<2><<<ga, 256, 0, s>>>(pa);
-    k_pack_split<2><<<gb, 256, 0, s>>>(pb);
-  } else {
-    k_pack_split<3><<<ga, 256, 0, s>>>(pa);
-    k_pack_split<3><<<gb, 256, 0, s>>>(pb);
+  if (ctab) {
+    pa.c_tab = ctab;
+    pb.c_tab = ctab + g.M;
+    for (int i = 0; i < g.nm; ++i) pa.c_str[i] = g.m_sc[i];
+    for (int i = 0; i < g.nn; ++i) pb.c_str[i] = g.n_sc[i];
   }
-  count_launch(2);
+  const int64_t units = g.L * (TM + TN) * NKT + (ctab ? (g.M + 255) / 256 + (g.N + 255) / 256 : 0);
+  const unsigned gp = (unsigned)std::min<int64_t>(units, (int64_t)num_sms * 8);
+  if (nterms == 2) k_pack_split<2><<<gp, 256, 0, s>>>(pa, pb);
+  else k_pack_split<3><<<gp, 256, 0, s>>>(pa, pb);
+  count_launch();
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
 
   PkArgs t;
   memset(&t, 0, sizeof(t));
   t.g = g;
+  if (ctab) {
+    t.g.m_tab_c = ctab;
+    t.g.n_tab_c = ctab + g.M;
+  }
   t.PA = PA;
   t.PB = PB;
   t.partial = part;
@@ -985,17 +1043,16 @@ cudaError_t launch_gemm_packed(const GemmArgs& g, int nterms, void* workspace, s
   const unsigned grid = (unsigned)std::min<int64_t>(t.units, G);
   {
     KernelTimer kt(s, "k_gemm_packed");
-    if (nterms == 2) k_gemm_packed<2><<<grid, NTHREADS, Cfg<2>::SMEM_BYTES, s>>>(t);
-    else k_gemm_packed<3><<<grid, NTHREADS, Cfg<3>::SMEM_BYTES, s>>>(t);
+    e = nterms == 2 ? launch_pdl(k_gemm_packed<2>, grid, NTHREADS, Cfg<2>::SMEM_BYTES, s, t)
+                    : launch_pdl(k_gemm_packed<3>, grid, NTHREADS, Cfg<3>::SMEM_BYTES, s, t);
   }
   count_launch();
-  e = cudaGetLastError();
   if (e != cudaSuccess || Rt == 0) return e;
   const int64_t total = Rt * BM * BN;
   const int64_t nb = (total + 255) / 256;
-  k_splitk_tiles<<<(unsigned)std::min<int64_t>(nb, (int64_t)num_sms * 16), 256, 0, s>>>(t);
+  e = launch_pdl(k_splitk_tiles, (unsigned)std::min<int64_t>(nb, (int64_t)num_sms * 16), 256, 0, s, t);
   count_launch();
-  return cudaGetLastError();
+  return e;
 }
 
 // One thread waits on an mbarrier that nothing arrives on, bounded by

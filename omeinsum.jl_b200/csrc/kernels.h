@@ -78,9 +78,11 @@ bool gemm_split_supported(const GemmArgs& g);
 // g.m_tab_c / g.n_tab_c at them (for mode groups of several modes).
 cudaError_t launch_c_offsets(GemmArgs& g, int64_t* tab, cudaStream_t s);
 // Pre-split (packed BF16 terms) + bulk-copy-fed persistent GEMM; needs
-// gemm_packed_bytes() of workspace, returns cudaErrorNotSupported otherwise.
+// gemm_packed_bytes() of workspace, returns cudaErrorNotSupported otherwise
+// (before launching anything).  ctab (M + N entries, or NULL): the C offset
+// tables, filled by the pack launch and used by the GEMM's epilogue.
 cudaError_t launch_gemm_packed(const GemmArgs& g, int nterms, void* workspace, size_t ws_bytes, int num_sms,
-                               cudaStream_t s);
+                               cudaStream_t s, int64_t* ctab);
 size_t gemm_packed_bytes(const GemmArgs& g, int nterms, int num_sms);
 
 // Synchronise s and read/clear the device timeout flag: 1 if a bounded wait
