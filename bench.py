@@ -364,12 +364,17 @@ def serve_section(ome, dev, njobs=32, rate=2000.0, seed=10, nmin=40, nmax=200, g
     ome.release_workspaces()
     torch.cuda.empty_cache()
     srv = ome.TNServer(n_slots=16, hbm_budget_bytes=150e9)
+    # one untimed pass of the same trace first (kernel loading, slot
+    # workspaces), then the measured one on the same server
+    srv.run_trace([ome.Job(j.code, j.xs, grad=j.grad, arrival=j.arrival, log2_scale=j.log2_scale) for j in jobs],
+                  timeout_s=cap_s)
     st = srv.run_trace(jobs, timeout_s=cap_s)
     srv.close()
     done = [j for j in jobs if j.done >= 0 and j.value is not None and j in srv.finished]
     st.update({"workload": f"{njobs} jobs, Poisson {rate:.0f}/s (seed {seed}), n uniform even [{nmin},{nmax}], "
                            "bond 2, unscaled FP32 normal(0,1), 10% gradient jobs, greedy order (best of 10) + greedy "
-                           "slicing to 2^27 (client side), 16 slots sharing a 150 GB workspace budget",
+                           "slicing to 2^27 (client side), 16 slots sharing a 150 GB workspace budget; measured "
+                           "after one untimed pass of the same trace",
                "submitted": njobs, "incomplete": njobs - len(done) - int(st.get("rejected", 0)), "cap_s": cap_s,
                "client_planning_s": plan_s, "n_of_completed": sorted(int(len(j.xs)) for j in done)})
     return st

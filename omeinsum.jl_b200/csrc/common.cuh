@@ -3,6 +3,7 @@
 // OMEinsum.jl (src/Core.jl:116-145 EinIndexer: offset = sum (i_d-1)*stride_d).
 #pragma once
 
+#include <utility>
 #include <cuda_runtime.h>
 #include <stdint.h>
 #include <math.h>
@@ -302,6 +303,32 @@ __host__ __device__ __forceinline__ int64_t mode_offset(int64_t i, int n, const 
     i = q;
   }
   return off;
+}
+
+// Programmatic dependent launch: a kernel launched with the programmatic
+// stream-serialisation attribute (launch_pdl) may start while the previous
+// kernel in its stream finishes; it runs its set-up, then waits in
+// griddep_wait until that kernel has completed and its writes are visible.
+// The previous kernel lets it start once all its own blocks are running
+// (griddep_launch_dependents).  Both are no-ops without the attribute.
+__device__ __forceinline__ void griddep_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void griddep_launch_dependents() {
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+template <class... KArgs, class... Args>
+static cudaError_t launch_pdl(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t s,
+                              Args&&... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
 }
 
 }  // namespace ome

@@ -30,7 +30,6 @@
 //    kernel records g_ome_timeout, stops waiting and frees its TMEM.
 #include <cuda_bf16.h>
 #include <string.h>
-#include <utility>
 #include "kernels.h"
 
 namespace ome {
@@ -591,15 +590,6 @@ struct PackArgs {
   int64_t r_ext[MAXG], r_str[MAXG], k_ext[MAXG], k_str[MAXG], l_ext[MAXG], l_str[MAXG], c_str[MAXG];
 };
 
-// Programmatic dependent launch: a kernel launched with the programmatic
-// stream-serialisation attribute may start while the previous kernel in its
-// stream finishes; it runs its set-up, then waits here until that kernel has
-// completed and its writes are visible.  The previous kernel lets it start
-// once all its own blocks are running.
-__device__ __forceinline__ void griddep_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
-__device__ __forceinline__ void griddep_launch_dependents() {
-  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
-}
 
 struct PkArgs {
   GemmArgs g;                  // C, M, N, L and the epilogue
@@ -649,7 +639,6 @@ __device__ __forceinline__ void pack_blob(const PackArgs& p, int64_t b, int warp
 template <int NT>
 __global__ void __launch_bounds__(256) k_pack_split(const __grid_constant__ PackArgs pa,
                                                     const __grid_constant__ PackArgs pb) {
-  griddep_launch_dependents();
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int64_t na = pa.L * pa.RT * pa.NKT, nb = pb.L * pb.RT * pb.NKT;
   const int64_t ta = pa.c_tab ? (pa.R + 255) / 256 : 0, tb = pb.c_tab ? (pb.R + 255) / 256 : 0;
@@ -726,9 +715,6 @@ __global__ void __launch_bounds__(pk::NTHREADS, 1) k_gemm_packed(const __grid_co
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
-  // the packs (and the offset tables) are complete from here on
-  griddep_wait();
-  griddep_launch_dependents();
   const uint32_t tmem = *tmem_slot;
   auto tmem_main = [&](int b) { return tmem + (uint32_t)(256 * b); };
   auto tmem_cross = [&](int b) { return tmem + (uint32_t)(256 * b + 128); };
@@ -896,7 +882,6 @@ __global__ void __launch_bounds__(pk::NTHREADS, 1) k_gemm_packed(const __grid_co
 // Sum the S split partials of each split tile in split order; αβ epilogue.
 __global__ void __launch_bounds__(256) k_splitk_tiles(const __grid_constant__ PkArgs t) {
   using namespace pk;
-  griddep_wait();
   const GemmArgs& g = t.g;
   const float sx = scalar_as<float>(g.sx), sy = scalar_as<float>(g.sy);
   float* Cp = static_cast<float*>(g.C);
@@ -946,23 +931,6 @@ size_t gemm_packed_bytes(const GemmArgs& g, int nterms, int num_sms) {
   const size_t blob = (size_t)nterms * TILE_BYTES;
   // packed operands + at most one grid's worth of split partials
   return (size_t)g.L * (TM + TN) * NKT * blob + (size_t)num_sms * BM * BN * 4 + 1024;
-}
-
-// Launch with programmatic stream serialisation (see griddep_wait).
-template <class... KArgs, class... Args>
-static cudaError_t launch_pdl(void (*kernel)(KArgs...), unsigned grid, unsigned block, size_t smem, cudaStream_t s,
-                              Args&&... args) {
-  cudaLaunchConfig_t cfg = {};
-  cfg.gridDim = dim3(grid);
-  cfg.blockDim = dim3(block);
-  cfg.dynamicSmemBytes = smem;
-  cfg.stream = s;
-  cudaLaunchAttribute at[1];
-  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-  at[0].val.programmaticStreamSerializationAllowed = 1;
-  cfg.attrs = at;
-  cfg.numAttrs = 1;
-  return cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
 }
 
 cudaError_t launch_gemm_packed(const GemmArgs& g, int nterms, void* workspace, size_t ws_bytes, int num_sms,
@@ -1041,18 +1009,21 @@ cudaError_t launch_gemm_packed(const GemmArgs& g, int nterms, void* workspace, s
   t.ksplit = ksplit;
   t.units = F + Rt * S;
   const unsigned grid = (unsigned)std::min<int64_t>(t.units, G);
+  // plain launches: a GEMM block started early would hold its SM's shared
+  // memory and TMEM while waiting, which stalls other streams' kernels
   {
     KernelTimer kt(s, "k_gemm_packed");
-    e = nterms == 2 ? launch_pdl(k_gemm_packed<2>, grid, NTHREADS, Cfg<2>::SMEM_BYTES, s, t)
-                    : launch_pdl(k_gemm_packed<3>, grid, NTHREADS, Cfg<3>::SMEM_BYTES, s, t);
+    if (nterms == 2) k_gemm_packed<2><<<grid, NTHREADS, Cfg<2>::SMEM_BYTES, s>>>(t);
+    else k_gemm_packed<3><<<grid, NTHREADS, Cfg<3>::SMEM_BYTES, s>>>(t);
   }
   count_launch();
+  e = cudaGetLastError();
   if (e != cudaSuccess || Rt == 0) return e;
   const int64_t total = Rt * BM * BN;
   const int64_t nb = (total + 255) / 256;
-  e = launch_pdl(k_splitk_tiles, (unsigned)std::min<int64_t>(nb, (int64_t)num_sms * 16), 256, 0, s, t);
+  k_splitk_tiles<<<(unsigned)std::min<int64_t>(nb, (int64_t)num_sms * 16), 256, 0, s>>>(t);
   count_launch();
-  return e;
+  return cudaGetLastError();
 }
 
 // One thread waits on an mbarrier that nothing arrives on, bounded by

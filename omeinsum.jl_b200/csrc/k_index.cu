@@ -215,6 +215,7 @@ struct InnerCursor {
 template <class A, int NIN>
 __global__ void __launch_bounds__(256) k_loop_block(const __grid_constant__ LoopArgs a) {
   using T = typename A::T;
+  griddep_launch_dependents();   // the finish pass (if any) may start its set-up
   constexpr int NI = NIN > 0 ? NIN : MAXIN;
   constexpr int U = 4;
   __shared__ T sh[32];
@@ -264,6 +265,7 @@ __global__ void __launch_bounds__(256) k_loop_block(const __grid_constant__ Loop
 template <class A>
 __global__ void __launch_bounds__(256) k_loop_finish(const __grid_constant__ LoopArgs a) {
   using T = typename A::T;
+  griddep_wait();   // the partials of the previous kernel
   const T sx = scalar_as<T>(a.sx), sy = scalar_as<T>(a.sy);
   for (int64_t o = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; o < a.n_out;
        o += (int64_t)gridDim.x * blockDim.x) {
@@ -290,6 +292,7 @@ __global__ void __launch_bounds__(256) k_loop_finish(const __grid_constant__ Loo
 template <class A, bool VEC, class I>
 __global__ void __launch_bounds__(256) k_reduce_contig(const __grid_constant__ LoopArgs a, int64_t rchunk,
                                                        FastDiv chdiv) {
+  griddep_launch_dependents();   // the finish pass (if any) may start its set-up
   using T = typename A::T;
   constexpr int V = VEC ? (16 / sizeof(T) > 0 ? 16 / sizeof(T) : 1) : 1;
   constexpr int U = 8;
@@ -412,7 +415,7 @@ cudaError_t launch_loop_finish(ome_dtype dt, const LoopArgs& a, cudaStream_t s) 
   const int64_t nb = (a.n_out + 255) / 256;
   const int grid = (int)(nb < 4096 ? nb : 4096);
   cudaError_t e = cudaErrorInvalidValue;
-  OME_DISPATCH(dt, ALG, k_loop_finish<ALG><<<grid, 256, 0, s>>>(a); count_launch(); e = cudaGetLastError());
+  OME_DISPATCH(dt, ALG, e = launch_pdl(k_loop_finish<ALG>, dim3(grid), dim3(256), 0, s, a); count_launch());
   return e;
 }
 

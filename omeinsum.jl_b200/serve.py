@@ -251,8 +251,11 @@ class TNServer:
         return sum(s.job is not None for s in self.slots)
 
     def run_trace(self, jobs: Sequence[Job], timeout_s: float = 600.0):
-        """Feed jobs at their arrival times (seconds from now) and run until all finish."""
+        """Feed jobs at their arrival times (seconds from now) and run until all
+        finish; the returned stats() cover this trace only (slots, contexts and
+        workspaces carry over from earlier traces)."""
         pending = deque(sorted(jobs, key=lambda j: j.arrival))
+        self.finished, self.rejected = [], []
         self.t0 = time.perf_counter()
         while pending or self.queue or any(s.job is not None for s in self.slots):
             now = self.clock()
