@@ -581,15 +581,17 @@ __global__ void __launch_bounds__(256) k_transpose_v4(const __grid_constant__ Tr
   const int sc4 = (threadIdx.x % SC) * 4, sr = threadIdx.x / SC;
   const T* x = static_cast<const T*>(a.x);
   T* y = static_cast<T*>(a.y);
-  for (uint32_t tid = blockIdx.x; tid < a.ntiles; tid += gridDim.x) {
+  // tile tid -> y-fast tile i0, x-fast tile it, batch offsets xb / yb
+  auto decode = [&](uint32_t tid, int32_t& i0, int32_t& it, int32_t& xb, int32_t& yb) {
     uint32_t rr = tid;
     uint32_t q = fast_div(rr, a.t0);
-    const int32_t i0 = (int32_t)(rr - q * a.t0.d);    // y-fast tile
+    i0 = (int32_t)(rr - q * a.t0.d);
     rr = q;
     q = fast_div(rr, a.tt);
-    const int32_t it = (int32_t)(rr - q * a.tt.d);    // x-fast tile
+    it = (int32_t)(rr - q * a.tt.d);
     rr = q;
-    int32_t xb = 0, yb = 0;
+    xb = 0;
+    yb = 0;
     for (int m = 0; m < a.nb; ++m) {
       q = fast_div(rr, a.bdiv[m]);
       const int32_t d = (int32_t)(rr - q * a.bdiv[m].d);
@@ -597,15 +599,26 @@ __global__ void __launch_bounds__(256) k_transpose_v4(const __grid_constant__ Tr
       xb += d * a.bxs[m];
       yb += d * a.bys[m];
     }
-    // load: rows = y-fast index (x stride xs0), float4 along x-fast p
+  };
+  // load: rows = y-fast index (x stride xs0), float4 along x-fast p
+  auto load = [&](int32_t i0, int32_t it, int32_t xb, uint4 (&v)[LP]) {
     const int32_t p = it * PW + lc4;
-    uint4 v[LP];
 #pragma unroll
     for (int k = 0; k < LP; ++k) {
       const int32_t qq = i0 * QH + lr + LR * k;
       if (p < a.et && qq < a.e0) v[k] = __ldg(reinterpret_cast<const uint4*>(x + xb + qq * a.xs0 + p));
       else v[k] = make_uint4(0, 0, 0, 0);
     }
+  };
+  uint32_t tid = blockIdx.x;
+  if (tid >= a.ntiles) return;
+  int32_t i0, it, xb, yb;
+  decode(tid, i0, it, xb, yb);
+  uint4 v[LP];
+  load(i0, it, xb, v);
+  // the next tile's loads are issued before this tile's stores, so a block
+  // always has reads in flight
+  for (; tid < a.ntiles; tid += gridDim.x) {
 #pragma unroll
     for (int k = 0; k < LP; ++k) {
       const T* e = reinterpret_cast<const T*>(&v[k]);
@@ -613,6 +626,12 @@ __global__ void __launch_bounds__(256) k_transpose_v4(const __grid_constant__ Tr
       for (int i = 0; i < 4; ++i) tile[lc4 + i][lr + LR * k] = e[i];
     }
     __syncthreads();
+    const uint32_t nt = tid + gridDim.x;
+    int32_t ni0 = 0, nit = 0, nxb = 0, nyb = 0;
+    if (nt < a.ntiles) {
+      decode(nt, ni0, nit, nxb, nyb);
+      load(ni0, nit, nxb, v);
+    }
     // store: rows = x-fast index (y stride yst), float4 along y-fast q
     const int32_t qs = i0 * QH + sc4;
 #pragma unroll
@@ -638,6 +657,10 @@ __global__ void __launch_bounds__(256) k_transpose_v4(const __grid_constant__ Tr
       }
     }
     __syncthreads();
+    i0 = ni0;
+    it = nit;
+    xb = nxb;
+    yb = nyb;
   }
 }
 
