@@ -301,14 +301,20 @@ static int run_loop(ome_ctx* ctx, cudaStream_t s, ome_dtype dt, int nin, const H
 
   const int sms = ctx->num_sms;
   // one input whose first summed mode is contiguous: row-vectorised reduction
-  if (nin == 1 && (inner.n == 1 || inner.n == 2) && inner.str[1][0] == 1 && inner.ext[0] >= 32 &&
-      n_out < (int64_t)sms * 2048) {
+  if (nin == 1 && (inner.n == 1 || inner.n == 2) && inner.str[1][0] == 1 && inner.ext[0] >= 32) {
     const int64_t R = inner.n == 2 ? inner.ext[1] : 1;
     const size_t es = dtype_size(dt);
     const int64_t V = (int64_t)(16 / es);
     bool vec = inner.ext[0] % V == 0 && ((uintptr_t)xu[0].data % 16) == 0;
     for (int m = 0; m < outer.n && vec; ++m) vec = (outer.str[1][m] * (int64_t)es) % 16 == 0;
     if (inner.n == 2) vec = vec && (inner.str[1][1] * (int64_t)es) % 16 == 0;
+    // many outputs: a warp per output
+    if (n_out >= (int64_t)sms * 64) {
+      const int grid = (int)std::min<int64_t>((n_out + 7) / 8, (int64_t)sms * 128);
+      trace_path("reduce_rows n_out=%lld n_in=%lld modes=%d+%d vec=%d", (long long)n_out, (long long)n_in,
+                 outer.n, inner.n, (int)vec);
+      return cuda_err(launch_reduce_rows(dt, a, vec, grid, s), "reduce kernel");
+    }
     int64_t nsplit = 1;
     const int64_t target = (int64_t)sms * 16;
     if (n_out < target) nsplit = std::min<int64_t>((target + n_out - 1) / n_out, R);

@@ -355,6 +355,76 @@ __global__ void __launch_bounds__(256) k_reduce_contig(const __grid_constant__ L
   }
 }
 
+// The same reduction when there are many outputs (column sums of a tall
+// column-major array, `ijk->jk`): one warp per output, lanes along the
+// contiguous row with 16-byte loads (4 per lane in flight), the optional
+// second summed mode as an outer loop, then a shuffle reduction.  Every lane
+// runs the same row and round counts, so the whole warp reaches the shuffles.
+template <class A, bool VEC>
+__global__ void __launch_bounds__(256) k_reduce_rows(const __grid_constant__ LoopArgs a) {
+  using T = typename A::T;
+  constexpr int V = VEC ? (16 / sizeof(T) > 0 ? 16 / sizeof(T) : 1) : 1;
+  constexpr int U = 4;
+  const T sx = scalar_as<T>(a.sx), sy = scalar_as<T>(a.sy);
+  const T* x = static_cast<const T*>(a.x[0]);
+  const int64_t e0 = a.ext[a.nout];
+  const int64_t R = a.ninner > 1 ? a.ext[a.nout + 1] : 1;
+  const int64_t rs = a.ninner > 1 ? a.str[1][a.nout + 1] : 0;
+  const int64_t chunks = e0 / V;
+  const int lane = threadIdx.x & 31;
+  const int64_t nw = (int64_t)gridDim.x * (blockDim.x >> 5);
+  for (int64_t o = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); o < a.n_out; o += nw) {
+    int64_t off[1];
+    const int64_t yoff = loop_outer_offsets<1>(a, o, off);
+    T acc = A::zero();
+    for (int64_t r = 0; r < R; ++r) {
+      const T* row = x + off[0] + r * rs;
+      for (int64_t c0 = lane; c0 - lane < chunks; c0 += 32 * U) {
+        T part[U][V];
+#pragma unroll
+        for (int j = 0; j < U; ++j) {
+          const int64_t c = c0 + 32 * j;
+          if (c < chunks) {
+            if constexpr (VEC) {
+              const uint4 w = __ldg(reinterpret_cast<const uint4*>(row + c * V));
+              memcpy(&part[j][0], &w, sizeof(w));
+            } else {
+              part[j][0] = row[c];
+            }
+          } else {
+#pragma unroll
+            for (int v = 0; v < V; ++v) part[j][v] = A::zero();
+          }
+        }
+#pragma unroll
+        for (int j = 0; j < U; ++j)
+#pragma unroll
+          for (int v = 0; v < V; ++v) acc = A::add(acc, part[j][v]);
+      }
+    }
+    for (int d = 16; d > 0; d >>= 1) acc = A::add(acc, shfl_down_any(acc, d));
+    if (lane == 0) {
+      T* yp = static_cast<T*>(a.y) + yoff;
+      *yp = epilogue<A>(acc, yp, sx, sy, a.sy_zero, a.sx_one);
+    }
+  }
+}
+
+template <class A>
+static cudaError_t launch_reduce_rows_t(const LoopArgs& a, bool vec, int grid, cudaStream_t s) {
+  KernelTimer kt(s, "k_reduce_rows");
+  if (vec) k_reduce_rows<A, true><<<grid, 256, 0, s>>>(a);
+  else k_reduce_rows<A, false><<<grid, 256, 0, s>>>(a);
+  count_launch();
+  return cudaGetLastError();
+}
+
+cudaError_t launch_reduce_rows(ome_dtype dt, const LoopArgs& a, bool vec, int grid, cudaStream_t s) {
+  cudaError_t e = cudaErrorInvalidValue;
+  OME_DISPATCH(dt, ALG, e = launch_reduce_rows_t<ALG>(a, vec, grid, s));
+  return e;
+}
+
 template <class A>
 static cudaError_t launch_reduce_contig_t(const LoopArgs& a, bool vec, int64_t rchunk, int grid, cudaStream_t s) {
   const int64_t R = a.ninner > 1 ? a.ext[a.nout + 1] : 1;

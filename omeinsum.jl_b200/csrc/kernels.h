@@ -34,6 +34,8 @@ cudaError_t launch_loop_finish(ome_dtype dt, const LoopArgs& a, cudaStream_t s);
 // per (output, row split) with vector loads (vec) over rows of rchunk.
 cudaError_t launch_reduce_contig(ome_dtype dt, const LoopArgs& a, bool vec, int64_t rchunk, int grid,
                                  cudaStream_t s);
+// The same with one warp per output (many outputs).
+cudaError_t launch_reduce_rows(ome_dtype dt, const LoopArgs& a, bool vec, int grid, cudaStream_t s);
 
 // Permute / broadcast / identity copy with the αβ epilogue.
 cudaError_t launch_perm(ome_dtype dt, const PermArgs& a, int num_sms, cudaStream_t s);

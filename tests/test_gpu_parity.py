@@ -234,6 +234,29 @@ def test_packed_gemm_overflow_scratch():
 
 @pytest.mark.parametrize("dt", ["f32", "f64", "c64", "i64", "trop", "bool"])
 @pytest.mark.parametrize("code,sizes", [
+    ("ijk->jk", dict(i=64, j=96, k=160)),          # 15360 outputs of 64 contiguous elements: 16-byte loads
+    ("ijk->jk", dict(i=37, j=100, k=100)),         # rows of 37: element loads
+    ("ijkl->jl", dict(i=40, j=50, k=6, l=200)),    # a second summed mode (strided rows)
+])
+def test_sum_many_outputs(code, sizes, dt):
+    """Sum over a contiguous leading mode with many outputs (one warp per
+    output), and y <- 3y + 2f for Int64."""
+    rng = np.random.default_rng(14)
+    ixs, iy = parse(code)
+    xs = [gen(rng, [sizes[l] for l in ix], dt) for ix in ixs]
+    c = ome.EinCode(ixs, iy)
+    got = to_np(ome.einsum(c, [to_dev(x, dt) for x in xs], sizes))
+    ome.device_status()
+    assert_match(got, oracle(ixs, iy, xs, sizes, dt), dt)
+    if dt == "i64":
+        y0 = gen(rng, [sizes[l] for l in iy], dt)
+        yd = to_dev(y0, dt)
+        ome.einsum_(c, [to_dev(x, dt) for x in xs], yd, 2, 3, sizes)
+        assert_match(to_np(yd), 2 * oracle(ixs, iy, xs, sizes, dt) + 3 * y0, dt)
+
+
+@pytest.mark.parametrize("dt", ["f32", "f64", "c64", "i64", "trop", "bool"])
+@pytest.mark.parametrize("code,sizes", [
     ("bij,bjk->bik", dict(b=100, i=37, j=50, k=23)),     # ragged batch warp, partial 16x16 tiles
     ("bij,bkj->bki", dict(b=64, i=64, j=9, k=64)),        # transposed operands, full tiles
     ("bcij,bcjk->bcik", dict(b=40, c=3, i=5, j=7, k=6)),  # two batch modes, b innermost
