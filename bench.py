@@ -625,7 +625,7 @@ def main():
             detail[nm]["TFLOP/s"] = f / (ms / 1e3) / 1e12
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": "contractions/s", "n_gpus": world, "steps": args.steps,
-                "warmup": nw, "ms_per_step": step_ms_max, "higher_is_better": True,
+                "warmup": args.warmup, "warmup_steps_run": nw, "ms_per_step": step_ms_max, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded normal(0,1))",
                 "config": {"workload": WORKLOAD,
                            "l2": "flushed before every contraction (outside its events) by a 256 MiB write "

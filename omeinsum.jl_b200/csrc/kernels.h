@@ -49,7 +49,8 @@ cudaError_t launch_gemm_simt(ome_dtype dt, const GemmArgs& g, cudaStream_t s);
 // FP32 batched GEMM with M, N <= 64 on CUDA cores (64 x 64 tiles, one per batch).
 cudaError_t launch_gemm_simt_small_f32(const GemmArgs& g, cudaStream_t s);
 // Batched GEMM with the batch mode contiguous in A, B and C and M, N <= 64
-// (lanes = consecutive batches); cudaErrorNotSupported if the shape differs.
+// (4 consecutive batches per CTA staged in shared memory, k_gemm_bstage);
+// cudaErrorNotSupported if the shape differs.
 bool gemm_bfast_applies(const GemmArgs& g);
 cudaError_t launch_gemm_bfast(ome_dtype dt, const GemmArgs& g, cudaStream_t s);
 
