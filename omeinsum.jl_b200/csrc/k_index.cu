@@ -680,29 +680,16 @@ __global__ void __launch_bounds__(256) k_transpose_v4(const __grid_constant__ Tr
       else v[k] = make_uint4(0, 0, 0, 0);
     }
   };
-  uint32_t tid = blockIdx.x;
-  if (tid >= a.ntiles) return;
-  int32_t i0, it, xb, yb;
-  decode(tid, i0, it, xb, yb);
-  uint4 v[LP];
-  load(i0, it, xb, v);
-  // the next tile's loads are issued before this tile's stores, so a block
-  // always has reads in flight
-  for (; tid < a.ntiles; tid += gridDim.x) {
+  auto put = [&](const uint4 (&v)[LP]) {
 #pragma unroll
     for (int k = 0; k < LP; ++k) {
       const T* e = reinterpret_cast<const T*>(&v[k]);
 #pragma unroll
       for (int i = 0; i < 4; ++i) tile[lc4 + i][lr + LR * k] = e[i];
     }
-    __syncthreads();
-    const uint32_t nt = tid + gridDim.x;
-    int32_t ni0 = 0, nit = 0, nxb = 0, nyb = 0;
-    if (nt < a.ntiles) {
-      decode(nt, ni0, nit, nxb, nyb);
-      load(ni0, nit, nxb, v);
-    }
-    // store: rows = x-fast index (y stride yst), float4 along y-fast q
+  };
+  // store: rows = x-fast index (y stride yst), float4 along y-fast q
+  auto store = [&](int32_t i0, int32_t it, int32_t yb) {
     const int32_t qs = i0 * QH + sc4;
 #pragma unroll
     for (int k = 0; k < SP; ++k) {
@@ -726,11 +713,46 @@ __global__ void __launch_bounds__(256) k_transpose_v4(const __grid_constant__ Tr
         *reinterpret_cast<uint4*>(yp) = w;
       }
     }
-    __syncthreads();
-    i0 = ni0;
-    it = nit;
-    xb = nxb;
-    yb = nyb;
+  };
+  if constexpr (PW == 64) {
+    // 256-byte rows: the next tile's loads are issued before this tile's
+    // stores, so a block always has reads in flight (6% faster on 2- to
+    // 4-mode transposes than loading at the top of the loop)
+    uint32_t tid = blockIdx.x;
+    if (tid >= a.ntiles) return;
+    int32_t i0, it, xb, yb;
+    decode(tid, i0, it, xb, yb);
+    uint4 v[LP];
+    load(i0, it, xb, v);
+    for (; tid < a.ntiles; tid += gridDim.x) {
+      put(v);
+      __syncthreads();
+      const uint32_t nt = tid + gridDim.x;
+      int32_t ni0 = 0, nit = 0, nxb = 0, nyb = 0;
+      if (nt < a.ntiles) {
+        decode(nt, ni0, nit, nxb, nyb);
+        load(ni0, nit, nxb, v);
+      }
+      store(i0, it, yb);
+      __syncthreads();
+      i0 = ni0;
+      it = nit;
+      xb = nxb;
+      yb = nyb;
+    }
+  } else {
+    // 128-byte rows (a tile's 64 x rows each hit their own DRAM page): the
+    // early loads cost 3% here, so each tile loads at the top of the loop
+    for (uint32_t tid = blockIdx.x; tid < a.ntiles; tid += gridDim.x) {
+      int32_t i0, it, xb, yb;
+      decode(tid, i0, it, xb, yb);
+      uint4 v[LP];
+      load(i0, it, xb, v);
+      put(v);
+      __syncthreads();
+      store(i0, it, yb);
+      __syncthreads();
+    }
   }
 }
 
