@@ -273,6 +273,27 @@ static int run_loop(ome_ctx* ctx, cudaStream_t s, ome_dtype dt, int nin, const H
   if (n_out == 0) return OME_OK;
   outer.normalize(0);
   inner.normalize(1);
+  // one contiguous summed run per output and too few outputs to fill the
+  // GPU (`ijk->k` once i and j merge): view the run as rows (a divisor of its
+  // length in [512, 4096], a multiple of 16 if there is one) so that the
+  // row-split reduction spreads each output over many blocks
+  if (nin == 1 && inner.n == 1 && inner.str[1][0] == 1 && inner.ext[0] >= 16384 &&
+      n_out < (int64_t)ctx->num_sms * 16 && outer.n + 2 <= MAXM) {
+    const int64_t E = inner.ext[0];
+    int64_t row = 0;
+    for (int pass = 0; pass < 2 && !row; ++pass)
+      for (int64_t r = 4096; r >= 512; --r)
+        if (E % r == 0 && (pass == 1 || r % 16 == 0)) {
+          row = r;
+          break;
+        }
+    if (row) {
+      inner.n = 2;
+      inner.ext[0] = row;
+      inner.ext[1] = E / row;
+      for (int t = 0; t < inner.nt; ++t) inner.str[t][1] = inner.str[t][0] * row;
+    }
+  }
   if (outer.n + inner.n > MAXM)
     return set_err(OME_UNSUPPORTED, "index kernel: %d modes after merging exceed %d", outer.n + inner.n, MAXM);
 

@@ -234,6 +234,30 @@ def test_packed_gemm_overflow_scratch():
 
 @pytest.mark.parametrize("dt", ["f32", "f64", "c64", "i64", "trop", "bool"])
 @pytest.mark.parametrize("code,sizes", [
+    ("ijk->k", dict(i=64, j=512, k=8)),            # i, j merge into one run of 32768: cut into rows
+    ("ij->j", dict(i=100000, j=3)),                # run of 100000 = 25 rows of 4000
+    ("ij->j", dict(i=16411, j=5)),                 # prime run: no row length divides it
+])
+def test_sum_few_outputs_long_runs(code, sizes, dt):
+    """Sum of one long contiguous run per output with few outputs (the run
+    is viewed as rows so that the split reduction can spread it), and
+    y <- 3y + 2f for Int64."""
+    rng = np.random.default_rng(15)
+    ixs, iy = parse(code)
+    xs = [gen(rng, [sizes[l] for l in ix], dt) for ix in ixs]
+    c = ome.EinCode(ixs, iy)
+    got = to_np(ome.einsum(c, [to_dev(x, dt) for x in xs], sizes))
+    ome.device_status()
+    assert_match(got, oracle(ixs, iy, xs, sizes, dt), dt)
+    if dt == "i64":
+        y0 = gen(rng, [sizes[l] for l in iy], dt)
+        yd = to_dev(y0, dt)
+        ome.einsum_(c, [to_dev(x, dt) for x in xs], yd, 2, 3, sizes)
+        assert_match(to_np(yd), 2 * oracle(ixs, iy, xs, sizes, dt) + 3 * y0, dt)
+
+
+@pytest.mark.parametrize("dt", ["f32", "f64", "c64", "i64", "trop", "bool"])
+@pytest.mark.parametrize("code,sizes", [
     ("ijk->jk", dict(i=64, j=96, k=160)),          # 15360 outputs of 64 contiguous elements: 16-byte loads
     ("ijk->jk", dict(i=37, j=100, k=100)),         # rows of 37: element loads
     ("ijkl->jl", dict(i=40, j=50, k=6, l=200)),    # a second summed mode (strided rows)
