@@ -321,6 +321,12 @@ static int run_loop(ome_ctx* ctx, cudaStream_t s, ome_dtype dt, int nin, const H
   a.nsplit = 1;
 
   const int sms = ctx->num_sms;
+  // no summed labels (Hadamard and outer products, broadcast products): rows
+  // of y's fastest mode
+  if (inner.n == 0 && outer.n >= 1) {
+    trace_path("map_rows nin=%d n_out=%lld modes=%d", nin, (long long)n_out, outer.n);
+    return cuda_err(launch_map_rows(dt, a, sms, s), "map kernel");
+  }
   // one input whose first summed mode is contiguous: row-vectorised reduction
   if (nin == 1 && (inner.n == 1 || inner.n == 2) && inner.str[1][0] == 1 && inner.ext[0] >= 32) {
     const int64_t R = inner.n == 2 ? inner.ext[1] : 1;
@@ -354,6 +360,32 @@ static int run_loop(ome_ctx* ctx, cudaStream_t s, ome_dtype dt, int nin, const H
                (long long)n_in, outer.n, inner.n, (long long)nsplit, (int)vec);
     OME_CK(cuda_err(launch_reduce_contig(dt, a, vec, rchunk, grid, s), "reduce kernel"));
     if (nsplit > 1) OME_CK(cuda_err(launch_loop_finish(dt, a, s), "reduce finish"));
+    return OME_OK;
+  }
+  // summed modes strided while y's fastest mode is contiguous in the first
+  // input (GEMV `ij,j->i`, `ijk->ik`): a thread per output along that mode,
+  // coalesced across the warp, the summed space split over enough ranges to
+  // give every SM 8 blocks
+  if (inner.n >= 1 && outer.n >= 1 && outer.str[1][0] == 1 && inner.str[1][0] != 1 && n_in > 16 && n_out >= 256) {
+    const int64_t bx = (n_out + 255) / 256;
+    const int64_t target = (int64_t)sms * 8;
+    int64_t nsplit = 1;
+    if (bx < target) nsplit = std::min<int64_t>((target + bx - 1) / bx, std::max<int64_t>(1, n_in / 64));
+    int64_t chunk = (n_in + nsplit - 1) / nsplit;
+    nsplit = (n_in + chunk - 1) / chunk;
+    if (nsplit > 1) {
+      a.partial = ws_alloc(ctx, (size_t)(n_out * nsplit) * dtype_size(dt));
+      if (!a.partial) {
+        nsplit = 1;
+        chunk = n_in;
+      }
+    }
+    a.nsplit = (int)nsplit;
+    const dim3 grid((unsigned)std::min<int64_t>(bx, (int64_t)sms * 32), (unsigned)nsplit);
+    trace_path("loop_cols nin=%d n_out=%lld n_in=%lld modes=%d+%d nsplit=%lld", nin, (long long)n_out,
+               (long long)n_in, outer.n, inner.n, (long long)nsplit);
+    OME_CK(cuda_err(launch_loop_cols(dt, a, chunk, grid, s), "index kernel"));
+    if (nsplit > 1) OME_CK(cuda_err(launch_loop_finish(dt, a, s), "index kernel finish"));
     return OME_OK;
   }
   const bool thread_mode = n_in <= 16 || n_out >= (int64_t)sms * 512;

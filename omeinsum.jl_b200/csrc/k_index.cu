@@ -174,6 +174,98 @@ __global__ void __launch_bounds__(256) k_loop_thread(const __grid_constant__ Loo
   }
 }
 
+// Sum-products whose summed modes are strided while y's fastest mode is
+// contiguous in the inputs (GEMV `ij,j->i`, `ijk->ik`): a thread per output,
+// consecutive threads on consecutive outputs (each load is coalesced across
+// the warp), the summed space cut into nsplit ranges (blockIdx.y), each
+// walked by an odometer; split partials go to a.partial[o * nsplit + s] for
+// k_loop_finish.
+template <class A, int NIN>
+__global__ void __launch_bounds__(256) k_loop_cols(const __grid_constant__ LoopArgs a, int64_t chunk) {
+  using T = typename A::T;
+  constexpr int NI = NIN > 0 ? NIN : MAXIN;
+  const int nin = NIN > 0 ? NIN : a.nin;
+  const T sx = scalar_as<T>(a.sx), sy = scalar_as<T>(a.sy);
+  griddep_launch_dependents();
+  const int64_t split = blockIdx.y;
+  const int64_t jb = split * chunk;
+  const int64_t je = min(a.n_in, jb + chunk);
+  for (int64_t o = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; o < a.n_out;
+       o += (int64_t)gridDim.x * blockDim.x) {
+    int64_t off[NI];
+    const int64_t yoff = loop_outer_offsets<NIN>(a, o, off);
+    int64_t dig[MAXM];
+    int64_t j = jb;
+    for (int m = 0; m < a.ninner; ++m) {
+      const int mm = a.nout + m;
+      const int64_t e = a.ext[mm];
+      const int64_t q = j / e;
+      dig[m] = j - q * e;
+      j = q;
+#pragma unroll
+      for (int i = 0; i < NI; ++i)
+        if (i < nin) off[i] += dig[m] * a.str[1 + i][mm];
+    }
+    // U steps at a time: the odometer first records the U offsets, then all
+    // their loads are issued, then they are added in order (the sum order is
+    // the sequential one)
+    constexpr int U = 8;
+    T acc = A::zero();
+    for (int64_t jj = jb; jj < je; jj += U) {
+      int64_t o2[U][NI];
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+#pragma unroll
+        for (int i = 0; i < NI; ++i) o2[u][i] = off[i];
+        if (jj + u + 1 < je) {
+          for (int m = 0; m < a.ninner; ++m) {
+            const int mm = a.nout + m;
+#pragma unroll
+            for (int i = 0; i < NI; ++i)
+              if (i < nin) off[i] += a.str[1 + i][mm];
+            if (++dig[m] < a.ext[mm]) break;
+#pragma unroll
+            for (int i = 0; i < NI; ++i)
+              if (i < nin) off[i] -= a.ext[mm] * a.str[1 + i][mm];
+            dig[m] = 0;
+          }
+        }
+      }
+      T v[U];
+#pragma unroll
+      for (int u = 0; u < U; ++u) v[u] = jj + u < je ? loop_prod<A, NIN>(a, o2[u]) : A::zero();
+#pragma unroll
+      for (int u = 0; u < U; ++u)
+        if (jj + u < je) acc = A::add(acc, v[u]);
+    }
+    if (a.nsplit == 1) {
+      T* yp = static_cast<T*>(a.y) + yoff;
+      *yp = epilogue<A>(acc, yp, sx, sy, a.sy_zero, a.sx_one);
+    } else {
+      static_cast<T*>(a.partial)[o * a.nsplit + split] = acc;
+    }
+  }
+}
+
+template <class A>
+static cudaError_t launch_loop_cols_t(const LoopArgs& a, int64_t chunk, dim3 grid, cudaStream_t s) {
+  KernelTimer kt(s, "k_loop_cols");
+  switch (a.nin) {
+    case 1: k_loop_cols<A, 1><<<grid, 256, 0, s>>>(a, chunk); break;
+    case 2: k_loop_cols<A, 2><<<grid, 256, 0, s>>>(a, chunk); break;
+    case 3: k_loop_cols<A, 3><<<grid, 256, 0, s>>>(a, chunk); break;
+    default: k_loop_cols<A, 0><<<grid, 256, 0, s>>>(a, chunk); break;
+  }
+  count_launch();
+  return cudaGetLastError();
+}
+
+cudaError_t launch_loop_cols(ome_dtype dt, const LoopArgs& a, int64_t chunk, dim3 grid, cudaStream_t s) {
+  cudaError_t e = cudaErrorInvalidValue;
+  OME_DISPATCH(dt, ALG, e = launch_loop_cols_t<ALG>(a, chunk, grid, s));
+  return e;
+}
+
 // Inner counter advanced by a fixed step given as mixed-radix digits.
 template <int NIN>
 struct InnerCursor {
@@ -449,6 +541,148 @@ cudaError_t launch_reduce_contig(ome_dtype dt, const LoopArgs& a, bool vec, int6
                                  cudaStream_t s) {
   cudaError_t e = cudaErrorInvalidValue;
   OME_DISPATCH(dt, ALG, e = launch_reduce_contig_t<ALG>(a, vec, rchunk, grid, s));
+  return e;
+}
+
+// Contractions without summed labels (Hadamard and outer products,
+// broadcast products, Repeat copies): y = sx * (x1 * x2 * ...) (+ sy * y),
+// products left to right.  A block takes a segment of one row of y's fastest
+// mode (mode 0); the row's offsets come from one mixed-radix decomposition
+// per segment instead of one per element.  VEC: mode 0 has stride 1 in y and
+// stride 0 or 1 in every input, and all row starts it touches are 16-byte
+// aligned (checked by the host): 16-byte loads and stores, a stride-0 input
+// read once per vector.
+constexpr int MAP_U = 4;   // vectors per thread per segment (at most)
+template <class A, int NIN, bool VEC>
+__global__ void __launch_bounds__(256) k_map_rows(const __grid_constant__ LoopArgs a, int64_t nseg, int nu) {
+  using T = typename A::T;
+  constexpr int V = VEC ? (int)(16 / sizeof(T)) : 1;
+  constexpr int NI = NIN > 0 ? NIN : MAXIN;
+  const int nin = NIN > 0 ? NIN : a.nin;
+  const T sx = scalar_as<T>(a.sx), sy = scalar_as<T>(a.sy);
+  const int64_t e0 = a.ext[0];
+  const int64_t items = (a.n_out / e0) * nseg;
+  for (int64_t w = blockIdx.x; w < items; w += gridDim.x) {
+    const int64_t r = w / nseg, sg = w - r * nseg;
+    int64_t yoff = 0, off[NI];
+#pragma unroll
+    for (int k = 0; k < NI; ++k) off[k] = 0;
+    int64_t q = r;
+    for (int m = 1; m < a.nout; ++m) {
+      const int64_t e = a.ext[m];
+      const int64_t qq = q / e;
+      const int64_t d = q - qq * e;
+      q = qq;
+      yoff += d * a.str[0][m];
+#pragma unroll
+      for (int k = 0; k < NI; ++k)
+        if (k < nin) off[k] += d * a.str[1 + k][m];
+    }
+    T* yr = static_cast<T*>(a.y) + yoff;
+    const int64_t ys = a.str[0][0];
+#pragma unroll
+    for (int u = 0; u < MAP_U; ++u) {
+      const int64_t i = (sg * nu * 256 + (int64_t)u * 256 + threadIdx.x) * V;
+      if (u >= nu || i >= e0) break;
+      T p[V];
+#pragma unroll
+      for (int k = 0; k < NI; ++k) {
+        if (k >= nin) break;
+        const T* xk = static_cast<const T*>(a.x[k]) + off[k];
+        const int64_t xs = a.str[1 + k][0];
+        T v[V];
+        if constexpr (VEC) {
+          if (xs == 0) {
+            const T c = xk[0];
+#pragma unroll
+            for (int j = 0; j < V; ++j) v[j] = c;
+          } else {
+            const uint4 w4 = __ldg(reinterpret_cast<const uint4*>(xk + i));
+            memcpy(v, &w4, sizeof(w4));
+          }
+        } else {
+          v[0] = xk[i * xs];
+        }
+#pragma unroll
+        for (int j = 0; j < V; ++j) p[j] = k == 0 ? v[j] : A::mul(p[j], v[j]);
+      }
+      if constexpr (VEC) {
+        T* yp = yr + i;
+        T old[V];
+        if (!a.sy_zero) {
+          const uint4 w4 = *reinterpret_cast<const uint4*>(yp);
+          memcpy(old, &w4, sizeof(w4));
+        }
+#pragma unroll
+        for (int j = 0; j < V; ++j) p[j] = epilogue<A>(p[j], old + j, sx, sy, a.sy_zero, a.sx_one);
+        uint4 w4;
+        memcpy(&w4, p, sizeof(w4));
+        *reinterpret_cast<uint4*>(yp) = w4;
+      } else {
+        T* yp = yr + i * ys;
+        *yp = epilogue<A>(p[0], yp, sx, sy, a.sy_zero, a.sx_one);
+      }
+    }
+  }
+}
+
+template <class A, bool VEC>
+static void launch_map_rows_v(const LoopArgs& a, int64_t nseg, int nu, int grid, cudaStream_t s) {
+  switch (a.nin) {
+    case 1: k_map_rows<A, 1, VEC><<<grid, 256, 0, s>>>(a, nseg, nu); break;
+    case 2: k_map_rows<A, 2, VEC><<<grid, 256, 0, s>>>(a, nseg, nu); break;
+    case 3: k_map_rows<A, 3, VEC><<<grid, 256, 0, s>>>(a, nseg, nu); break;
+    default: k_map_rows<A, 0, VEC><<<grid, 256, 0, s>>>(a, nseg, nu); break;
+  }
+  count_launch();
+}
+
+// VEC when the element size divides 16 bytes (at least 2 per vector), mode 0
+// is contiguous in y and contiguous or broadcast in every input, its extent is
+// a multiple of the vector and every row start it touches is 16-byte aligned.
+static bool map_vec_ok(const LoopArgs& a, size_t es) {
+  if (es > 8 || 16 % es != 0) return false;
+  const int64_t V = (int64_t)(16 / es);
+  if (a.str[0][0] != 1 || a.ext[0] % V != 0 || (uintptr_t)a.y % 16 != 0) return false;
+  for (int m = 1; m < a.nout; ++m)
+    if ((a.str[0][m] * (int64_t)es) % 16 != 0) return false;
+  for (int k = 0; k < a.nin; ++k) {
+    const int64_t xs = a.str[1 + k][0];
+    if (xs == 0) continue;
+    if (xs != 1 || (uintptr_t)a.x[k] % 16 != 0) return false;
+    for (int m = 1; m < a.nout; ++m)
+      if ((a.str[1 + k][m] * (int64_t)es) % 16 != 0) return false;
+  }
+  return true;
+}
+
+template <class A>
+static cudaError_t launch_map_rows_t(const LoopArgs& a, int num_sms, cudaStream_t s) {
+  const bool vec = map_vec_ok(a, sizeof(typename A::T));
+  const int64_t V = vec ? (int64_t)(16 / sizeof(typename A::T)) : 1;
+  const int64_t rows = a.n_out / a.ext[0];
+  // segments of MAP_U vectors per thread, or of one when that leaves fewer
+  // than 8 blocks per SM (short rows: a diagonal, a small tensor)
+  int nu = MAP_U;
+  if (rows * ((a.ext[0] + MAP_U * 256 * V - 1) / (MAP_U * 256 * V)) < (int64_t)num_sms * 8) nu = 1;
+  const int64_t seg = (int64_t)nu * 256 * V;
+  const int64_t nseg = (a.ext[0] + seg - 1) / seg;
+  const int64_t items = rows * nseg;
+  const int grid = (int)std::min<int64_t>(items, (int64_t)num_sms * 32);
+  KernelTimer kt(s, "k_map_rows");
+  if constexpr (sizeof(typename A::T) <= 8 && 16 % sizeof(typename A::T) == 0) {
+    if (vec) launch_map_rows_v<A, true>(a, nseg, nu, grid, s);
+    else launch_map_rows_v<A, false>(a, nseg, nu, grid, s);
+  } else {
+    launch_map_rows_v<A, false>(a, nseg, nu, grid, s);
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t launch_map_rows(ome_dtype dt, const LoopArgs& a, int num_sms, cudaStream_t s) {
+  if (a.n_out == 0) return cudaSuccess;
+  cudaError_t e = cudaErrorInvalidValue;
+  OME_DISPATCH(dt, ALG, e = launch_map_rows_t<ALG>(a, num_sms, s));
   return e;
 }
 
@@ -872,6 +1106,27 @@ static cudaError_t launch_perm_t(const PermArgs& a, int num_sms, cudaStream_t s)
     const int grid = (int)(nb < 1 ? 1 : (nb < maxgrid ? nb : maxgrid));
     KernelTimer kt(s, "k_copy_vec");
     k_copy_vec<A><<<grid, 256, 0, s>>>(a); count_launch();
+  } else if (a.nd >= 1) {
+    // general copy / broadcast (Repeat): the row kernel over y's fastest mode
+    LoopArgs l;
+    memset(&l, 0, sizeof(l));
+    l.x[0] = a.x;
+    l.y = a.y;
+    l.nin = 1;
+    l.nout = a.nd;
+    l.ninner = 0;
+    l.n_out = a.n;
+    l.n_in = 1;
+    for (int m = 0; m < a.nd; ++m) {
+      l.ext[m] = a.ext[m];
+      l.str[0][m] = a.ys[m];
+      l.str[1][m] = a.xs[m];
+    }
+    l.sx = a.sx;
+    l.sy = a.sy;
+    l.sy_zero = a.sy_zero;
+    l.sx_one = a.sx_one;
+    return launch_map_rows_t<A>(l, num_sms, s);
   } else {
     const int64_t nb = (a.n + 255) / 256;
     const int grid = (int)(nb < maxgrid ? nb : maxgrid);

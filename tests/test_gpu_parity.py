@@ -234,6 +234,31 @@ def test_packed_gemm_overflow_scratch():
 
 @pytest.mark.parametrize("dt", ["f32", "f64", "c64", "i64", "trop", "bool"])
 @pytest.mark.parametrize("code,sizes", [
+    ("ij,j->i", dict(i=300, j=200)),               # GEMV: summed mode strided, outputs contiguous
+    ("ijk->ik", dict(i=40, j=300, k=10)),          # middle sum
+    ("ij,j,j->i", dict(i=260, j=70)),              # three inputs
+    ("ijk,jk->i", dict(i=512, j=9, k=11)),         # two summed modes (odometer carries)
+])
+def test_strided_sums(code, sizes, dt):
+    """Sum-products whose summed modes are strided while the outputs are
+    contiguous (a thread per output, summed space split), and y <- 3y + 2f
+    for Int64."""
+    rng = np.random.default_rng(16)
+    ixs, iy = parse(code)
+    xs = [gen(rng, [sizes[l] for l in ix], dt) for ix in ixs]
+    c = ome.EinCode(ixs, iy)
+    got = to_np(ome.einsum(c, [to_dev(x, dt) for x in xs], sizes))
+    ome.device_status()
+    assert_match(got, oracle(ixs, iy, xs, sizes, dt), dt)
+    if dt == "i64":
+        y0 = gen(rng, [sizes[l] for l in iy], dt)
+        yd = to_dev(y0, dt)
+        ome.einsum_(c, [to_dev(x, dt) for x in xs], yd, 2, 3, sizes)
+        assert_match(to_np(yd), 2 * oracle(ixs, iy, xs, sizes, dt) + 3 * y0, dt)
+
+
+@pytest.mark.parametrize("dt", ["f32", "f64", "c64", "i64", "trop", "bool"])
+@pytest.mark.parametrize("code,sizes", [
     ("ijk->k", dict(i=64, j=512, k=8)),            # i, j merge into one run of 32768: cut into rows
     ("ij->j", dict(i=100000, j=3)),                # run of 100000 = 25 rows of 4000
     ("ij->j", dict(i=16411, j=5)),                 # prime run: no row length divides it
