@@ -277,8 +277,17 @@ static int run_loop(ome_ctx* ctx, cudaStream_t s, ome_dtype dt, int nin, const H
   // GPU (`ijk->k` once i and j merge): view the run as rows (a divisor of its
   // length in [512, 4096], a multiple of 16 if there is one) so that the
   // row-split reduction spreads each output over many blocks
-  if (nin == 1 && inner.n == 1 && inner.str[1][0] == 1 && inner.ext[0] >= 16384 &&
-      n_out < (int64_t)ctx->num_sms * 16 && outer.n + 2 <= MAXM) {
+  // inputs whose first summed mode has stride 0 or 1, at least one of them 1:
+  // the contiguous reductions below read rows of that mode
+  bool rowwise = nin <= 3 && inner.n >= 1;
+  bool any_unit = false;
+  for (int k = 0; k < nin && rowwise; ++k) {
+    rowwise = inner.str[1 + k][0] == 0 || inner.str[1 + k][0] == 1;
+    any_unit = any_unit || inner.str[1 + k][0] == 1;
+  }
+  rowwise = rowwise && any_unit;
+  if (rowwise && inner.n == 1 && inner.ext[0] >= 16384 && n_out < (int64_t)ctx->num_sms * 16 &&
+      outer.n + 2 <= MAXM) {
     const int64_t E = inner.ext[0];
     int64_t row = 0;
     for (int pass = 0; pass < 2 && !row; ++pass)
@@ -328,13 +337,17 @@ static int run_loop(ome_ctx* ctx, cudaStream_t s, ome_dtype dt, int nin, const H
     return cuda_err(launch_map_rows(dt, a, sms, s), "map kernel");
   }
   // one input whose first summed mode is contiguous: row-vectorised reduction
-  if (nin == 1 && (inner.n == 1 || inner.n == 2) && inner.str[1][0] == 1 && inner.ext[0] >= 32) {
+  if (rowwise && (inner.n == 1 || inner.n == 2) && inner.ext[0] >= 32) {
     const int64_t R = inner.n == 2 ? inner.ext[1] : 1;
     const size_t es = dtype_size(dt);
     const int64_t V = (int64_t)(16 / es);
-    bool vec = inner.ext[0] % V == 0 && ((uintptr_t)xu[0].data % 16) == 0;
-    for (int m = 0; m < outer.n && vec; ++m) vec = (outer.str[1][m] * (int64_t)es) % 16 == 0;
-    if (inner.n == 2) vec = vec && (inner.str[1][1] * (int64_t)es) % 16 == 0;
+    bool vec = inner.ext[0] % V == 0;
+    for (int k = 0; k < nin && vec; ++k) {
+      if (inner.str[1 + k][0] == 0) continue;   // read once per row
+      vec = ((uintptr_t)xu[k].data % 16) == 0;
+      for (int m = 0; m < outer.n && vec; ++m) vec = (outer.str[1 + k][m] * (int64_t)es) % 16 == 0;
+      if (inner.n == 2) vec = vec && (inner.str[1 + k][1] * (int64_t)es) % 16 == 0;
+    }
     // many outputs: a warp per output
     if (n_out >= (int64_t)sms * 64) {
       const int grid = (int)std::min<int64_t>((n_out + 7) / 8, (int64_t)sms * 128);

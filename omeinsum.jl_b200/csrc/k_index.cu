@@ -381,32 +381,64 @@ __global__ void __launch_bounds__(256) k_loop_finish(const __grid_constant__ Loo
 // elements x R rows (at most one more summed mode, row stride rs).  One block
 // per (output, row split); 16-byte vector loads when VEC (every row start
 // 16-byte aligned and E0 a multiple of the vector width), 4 loads in flight.
-template <class A, bool VEC, class I>
+// Values of the NIN inputs at one unit (V consecutive elements of a row):
+// inputs with stride 1 along the row are read (16-byte loads when VEC),
+// stride-0 inputs give their row value; the product is left to right.
+template <class A, int NIN, bool VEC, int V>
+__device__ __forceinline__ void row_unit(const typename A::T* const (&xr)[NIN], const int (&s0)[NIN], int64_t c,
+                                         typename A::T (&out)[V]) {
+  using T = typename A::T;
+#pragma unroll
+  for (int k = 0; k < NIN; ++k) {
+    T v[V];
+    if (s0[k] == 0) {
+      const T c0 = xr[k][0];
+#pragma unroll
+      for (int j = 0; j < V; ++j) v[j] = c0;
+    } else if constexpr (VEC) {
+      const uint4 w = __ldg(reinterpret_cast<const uint4*>(xr[k] + c * V));
+      memcpy(v, &w, sizeof(w));
+    } else {
+      v[0] = xr[k][c];
+    }
+#pragma unroll
+    for (int j = 0; j < V; ++j) out[j] = k == 0 ? v[j] : A::mul(out[j], v[j]);
+  }
+}
+
+template <class A, int NIN, bool VEC, class I>
 __global__ void __launch_bounds__(256) k_reduce_contig(const __grid_constant__ LoopArgs a, int64_t rchunk,
                                                        FastDiv chdiv) {
   griddep_launch_dependents();   // the finish pass (if any) may start its set-up
   using T = typename A::T;
   constexpr int V = VEC ? (16 / sizeof(T) > 0 ? 16 / sizeof(T) : 1) : 1;
-  constexpr int U = 8;
+  constexpr int U = NIN == 1 ? 8 : 4;
   __shared__ T sh[32];
   const T sx = scalar_as<T>(a.sx), sy = scalar_as<T>(a.sy);
-  const T* x = static_cast<const T*>(a.x[0]);
   const int64_t e0 = a.ext[a.nout];
   const int64_t R = a.ninner > 1 ? a.ext[a.nout + 1] : 1;
-  const int64_t rs = a.ninner > 1 ? a.str[1][a.nout + 1] : 0;
+  int s0[NIN];
+  int64_t rs[NIN];
+#pragma unroll
+  for (int k = 0; k < NIN; ++k) {
+    s0[k] = (int)a.str[1 + k][a.nout];
+    rs[k] = a.ninner > 1 ? a.str[1 + k][a.nout + 1] : 0;
+  }
   const int64_t chunks = e0 / V;              // vector units per row
   const int64_t nblocks = a.n_out * a.nsplit;
   for (int64_t b = blockIdx.x; b < nblocks; b += gridDim.x) {
     const int64_t o = b / a.nsplit;
     const int64_t split = b - o * a.nsplit;
-    int64_t off[1];
-    const int64_t yoff = loop_outer_offsets<1>(a, o, off);
+    int64_t off[NIN];
+    const int64_t yoff = loop_outer_offsets<NIN>(a, o, off);
     const int64_t rbeg = split * rchunk;
     const int64_t rend = min(R, rbeg + rchunk);
     // offsets inside one split in I (int32 when the split's span fits)
     const I units = (I)((rend - rbeg) * chunks);
-    const I ich = (I)chunks, irs = (I)rs;
-    const T* xb = x + off[0] + rbeg * rs;
+    const I ich = (I)chunks;
+    const T* xb[NIN];
+#pragma unroll
+    for (int k = 0; k < NIN; ++k) xb[k] = static_cast<const T*>(a.x[k]) + off[k] + rbeg * rs[k];
     T acc = A::zero();
     for (I u0 = threadIdx.x; u0 < units; u0 += (I)blockDim.x * U) {
       T part[U][V];
@@ -418,13 +450,10 @@ __global__ void __launch_bounds__(256) k_reduce_contig(const __grid_constant__ L
           if constexpr (sizeof(I) == 4) r = (I)fast_div((uint32_t)u, chdiv);
           else r = u / ich;
           const I c = u - r * ich;
-          const T* p = xb + (I)(r * irs) + (I)(c * V);
-          if constexpr (VEC) {
-            const uint4 w = __ldg(reinterpret_cast<const uint4*>(p));
-            memcpy(&part[j][0], &w, sizeof(w));
-          } else {
-            part[j][0] = p[0];
-          }
+          const T* xr[NIN];
+#pragma unroll
+          for (int k = 0; k < NIN; ++k) xr[k] = xb[k] + (I)(r * (I)rs[k]);
+          row_unit<A, NIN, VEC, V>(xr, s0, (int64_t)c, part[j]);
         } else {
 #pragma unroll
           for (int v = 0; v < V; ++v) part[j][v] = A::zero();
@@ -448,41 +477,44 @@ __global__ void __launch_bounds__(256) k_reduce_contig(const __grid_constant__ L
 }
 
 // The same reduction when there are many outputs (column sums of a tall
-// column-major array, `ijk->jk`): one warp per output, lanes along the
-// contiguous row with 16-byte loads (4 per lane in flight), the optional
-// second summed mode as an outer loop, then a shuffle reduction.  Every lane
-// runs the same row and round counts, so the whole warp reaches the shuffles.
-template <class A, bool VEC>
+// column-major array, `ijk->jk`; GEMV `ji,j->i`): one warp per output, lanes
+// along the contiguous row with 16-byte loads (4 per lane in flight), the
+// optional second summed mode as an outer loop, then a shuffle reduction.
+// Every lane runs the same row and round counts, so the whole warp reaches
+// the shuffles.
+template <class A, int NIN, bool VEC>
 __global__ void __launch_bounds__(256) k_reduce_rows(const __grid_constant__ LoopArgs a) {
   using T = typename A::T;
   constexpr int V = VEC ? (16 / sizeof(T) > 0 ? 16 / sizeof(T) : 1) : 1;
   constexpr int U = 4;
   const T sx = scalar_as<T>(a.sx), sy = scalar_as<T>(a.sy);
-  const T* x = static_cast<const T*>(a.x[0]);
   const int64_t e0 = a.ext[a.nout];
   const int64_t R = a.ninner > 1 ? a.ext[a.nout + 1] : 1;
-  const int64_t rs = a.ninner > 1 ? a.str[1][a.nout + 1] : 0;
+  int s0[NIN];
+  int64_t rs[NIN];
+#pragma unroll
+  for (int k = 0; k < NIN; ++k) {
+    s0[k] = (int)a.str[1 + k][a.nout];
+    rs[k] = a.ninner > 1 ? a.str[1 + k][a.nout + 1] : 0;
+  }
   const int64_t chunks = e0 / V;
   const int lane = threadIdx.x & 31;
   const int64_t nw = (int64_t)gridDim.x * (blockDim.x >> 5);
   for (int64_t o = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); o < a.n_out; o += nw) {
-    int64_t off[1];
-    const int64_t yoff = loop_outer_offsets<1>(a, o, off);
+    int64_t off[NIN];
+    const int64_t yoff = loop_outer_offsets<NIN>(a, o, off);
     T acc = A::zero();
     for (int64_t r = 0; r < R; ++r) {
-      const T* row = x + off[0] + r * rs;
+      const T* xr[NIN];
+#pragma unroll
+      for (int k = 0; k < NIN; ++k) xr[k] = static_cast<const T*>(a.x[k]) + off[k] + r * rs[k];
       for (int64_t c0 = lane; c0 - lane < chunks; c0 += 32 * U) {
         T part[U][V];
 #pragma unroll
         for (int j = 0; j < U; ++j) {
           const int64_t c = c0 + 32 * j;
           if (c < chunks) {
-            if constexpr (VEC) {
-              const uint4 w = __ldg(reinterpret_cast<const uint4*>(row + c * V));
-              memcpy(&part[j][0], &w, sizeof(w));
-            } else {
-              part[j][0] = row[c];
-            }
+            row_unit<A, NIN, VEC, V>(xr, s0, c, part[j]);
           } else {
 #pragma unroll
             for (int v = 0; v < V; ++v) part[j][v] = A::zero();
@@ -502,11 +534,18 @@ __global__ void __launch_bounds__(256) k_reduce_rows(const __grid_constant__ Loo
   }
 }
 
+template <class A, int NIN>
+static void launch_reduce_rows_n(const LoopArgs& a, bool vec, int grid, cudaStream_t s) {
+  if (vec) k_reduce_rows<A, NIN, true><<<grid, 256, 0, s>>>(a);
+  else k_reduce_rows<A, NIN, false><<<grid, 256, 0, s>>>(a);
+}
+
 template <class A>
 static cudaError_t launch_reduce_rows_t(const LoopArgs& a, bool vec, int grid, cudaStream_t s) {
   KernelTimer kt(s, "k_reduce_rows");
-  if (vec) k_reduce_rows<A, true><<<grid, 256, 0, s>>>(a);
-  else k_reduce_rows<A, false><<<grid, 256, 0, s>>>(a);
+  if (a.nin == 1) launch_reduce_rows_n<A, 1>(a, vec, grid, s);
+  else if (a.nin == 2) launch_reduce_rows_n<A, 2>(a, vec, grid, s);
+  else launch_reduce_rows_n<A, 3>(a, vec, grid, s);
   count_launch();
   return cudaGetLastError();
 }
@@ -517,22 +556,32 @@ cudaError_t launch_reduce_rows(ome_dtype dt, const LoopArgs& a, bool vec, int gr
   return e;
 }
 
+template <class A, int NIN>
+static void launch_reduce_contig_n(const LoopArgs& a, bool vec, bool small, int64_t rchunk, FastDiv chdiv, int grid,
+                                   cudaStream_t s) {
+  if (vec) {
+    if (small) k_reduce_contig<A, NIN, true, int32_t><<<grid, 256, 0, s>>>(a, rchunk, chdiv);
+    else k_reduce_contig<A, NIN, true, int64_t><<<grid, 256, 0, s>>>(a, rchunk, chdiv);
+  } else {
+    if (small) k_reduce_contig<A, NIN, false, int32_t><<<grid, 256, 0, s>>>(a, rchunk, chdiv);
+    else k_reduce_contig<A, NIN, false, int64_t><<<grid, 256, 0, s>>>(a, rchunk, chdiv);
+  }
+}
+
 template <class A>
 static cudaError_t launch_reduce_contig_t(const LoopArgs& a, bool vec, int64_t rchunk, int grid, cudaStream_t s) {
   const int64_t R = a.ninner > 1 ? a.ext[a.nout + 1] : 1;
-  const int64_t rs = a.ninner > 1 ? a.str[1][a.nout + 1] : 0;
-  const bool small = rchunk * (rs > 0 ? rs : 1) + a.ext[a.nout] < ((int64_t)1 << 30) &&
-                     R * a.ext[a.nout] < ((int64_t)1 << 30);
+  bool small = R * a.ext[a.nout] < ((int64_t)1 << 30);
+  for (int k = 0; k < a.nin; ++k) {
+    const int64_t rs = a.ninner > 1 ? a.str[1 + k][a.nout + 1] : 0;
+    small = small && rchunk * (rs > 0 ? rs : 1) + a.ext[a.nout] < ((int64_t)1 << 30);
+  }
   constexpr int V = 16 / sizeof(typename A::T) > 0 ? 16 / sizeof(typename A::T) : 1;
   const FastDiv chdiv = make_fastdiv((uint32_t)(small ? a.ext[a.nout] / (vec ? V : 1) : 1));
   KernelTimer kt(s, "k_reduce_contig");
-  if (vec) {
-    if (small) k_reduce_contig<A, true, int32_t><<<grid, 256, 0, s>>>(a, rchunk, chdiv);
-    else k_reduce_contig<A, true, int64_t><<<grid, 256, 0, s>>>(a, rchunk, chdiv);
-  } else {
-    if (small) k_reduce_contig<A, false, int32_t><<<grid, 256, 0, s>>>(a, rchunk, chdiv);
-    else k_reduce_contig<A, false, int64_t><<<grid, 256, 0, s>>>(a, rchunk, chdiv);
-  }
+  if (a.nin == 1) launch_reduce_contig_n<A, 1>(a, vec, small, rchunk, chdiv, grid, s);
+  else if (a.nin == 2) launch_reduce_contig_n<A, 2>(a, vec, small, rchunk, chdiv, grid, s);
+  else launch_reduce_contig_n<A, 3>(a, vec, small, rchunk, chdiv, grid, s);
   count_launch();
   return cudaGetLastError();
 }

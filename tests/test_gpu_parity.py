@@ -234,6 +234,32 @@ def test_packed_gemm_overflow_scratch():
 
 @pytest.mark.parametrize("dt", ["f32", "f64", "c64", "i64", "trop", "bool"])
 @pytest.mark.parametrize("code,sizes", [
+    ("ji,j->i", dict(i=12000, j=64)),              # GEMV with the summed mode contiguous: a warp per output
+    ("i,i->", dict(i=65536)),                      # dot: one long run cut into rows, split over blocks
+    ("ij,ij->j", dict(i=96, j=500)),               # batched dot, few outputs
+    ("ijk,ik->k", dict(i=64, j=30, k=20)),         # second input constant along the row mode j
+    ("ij,i,i->j", dict(i=33, j=40)),               # three inputs, rows not a multiple of the vector
+])
+def test_multi_input_contiguous_sums(code, sizes, dt):
+    """Sum-products whose first summed mode is contiguous (or constant) in
+    every input (dot products, GEMV with a contiguous row), and y <- 3y + 2f
+    for Int64."""
+    rng = np.random.default_rng(17)
+    ixs, iy = parse(code)
+    xs = [gen(rng, [sizes[l] for l in ix], dt) for ix in ixs]
+    c = ome.EinCode(ixs, iy)
+    got = to_np(ome.einsum(c, [to_dev(x, dt) for x in xs], sizes))
+    ome.device_status()
+    assert_match(got, oracle(ixs, iy, xs, sizes, dt), dt)
+    if dt == "i64":
+        y0 = gen(rng, [sizes[l] for l in iy], dt)
+        yd = to_dev(y0, dt)
+        ome.einsum_(c, [to_dev(x, dt) for x in xs], yd, 2, 3, sizes)
+        assert_match(to_np(yd), 2 * oracle(ixs, iy, xs, sizes, dt) + 3 * y0, dt)
+
+
+@pytest.mark.parametrize("dt", ["f32", "f64", "c64", "i64", "trop", "bool"])
+@pytest.mark.parametrize("code,sizes", [
     ("ij,j->i", dict(i=300, j=200)),               # GEMV: summed mode strided, outputs contiguous
     ("ijk->ik", dict(i=40, j=300, k=10)),          # middle sum
     ("ij,j,j->i", dict(i=260, j=70)),              # three inputs
