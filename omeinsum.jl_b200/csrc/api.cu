@@ -380,14 +380,27 @@ static int run_loop(ome_ctx* ctx, cudaStream_t s, ome_dtype dt, int nin, const H
   // coalesced across the warp, the summed space split over enough ranges to
   // give every SM 8 blocks
   if (inner.n >= 1 && outer.n >= 1 && outer.str[1][0] == 1 && inner.str[1][0] != 1 && n_in > 16 && n_out >= 256) {
-    const int64_t bx = (n_out + 255) / 256;
+    // 16-byte accesses along the outputs: y contiguous there, every input
+    // contiguous or constant there, all offsets the threads reach aligned
+    const size_t es = dtype_size(dt);
+    const int64_t V = es <= 8 && 16 % es == 0 ? (int64_t)(16 / es) : 1;
+    bool vec = V > 1 && outer.str[0][0] == 1 && outer.ext[0] % V == 0 && ((uintptr_t)yu.data % 16) == 0;
+    for (int m = 1; m < outer.n && vec; ++m) vec = (outer.str[0][m] * (int64_t)es) % 16 == 0;
+    for (int k = 0; k < nin && vec; ++k) {
+      const int64_t s0 = outer.str[1 + k][0];
+      if (s0 == 0) continue;
+      vec = s0 == 1 && ((uintptr_t)xu[k].data % 16) == 0;
+      for (int m = 1; m < outer.n && vec; ++m) vec = (outer.str[1 + k][m] * (int64_t)es) % 16 == 0;
+      for (int m = 0; m < inner.n && vec; ++m) vec = (inner.str[1 + k][m] * (int64_t)es) % 16 == 0;
+    }
+    const int64_t bx = (n_out / (vec ? V : 1) + 255) / 256;
     const int64_t target = (int64_t)sms * 8;
     int64_t nsplit = 1;
     if (bx < target) nsplit = std::min<int64_t>((target + bx - 1) / bx, std::max<int64_t>(1, n_in / 64));
     int64_t chunk = (n_in + nsplit - 1) / nsplit;
     nsplit = (n_in + chunk - 1) / chunk;
     if (nsplit > 1) {
-      a.partial = ws_alloc(ctx, (size_t)(n_out * nsplit) * dtype_size(dt));
+      a.partial = ws_alloc(ctx, (size_t)(n_out * nsplit) * es);
       if (!a.partial) {
         nsplit = 1;
         chunk = n_in;
@@ -395,9 +408,9 @@ static int run_loop(ome_ctx* ctx, cudaStream_t s, ome_dtype dt, int nin, const H
     }
     a.nsplit = (int)nsplit;
     const dim3 grid((unsigned)std::min<int64_t>(bx, (int64_t)sms * 32), (unsigned)nsplit);
-    trace_path("loop_cols nin=%d n_out=%lld n_in=%lld modes=%d+%d nsplit=%lld", nin, (long long)n_out,
-               (long long)n_in, outer.n, inner.n, (long long)nsplit);
-    OME_CK(cuda_err(launch_loop_cols(dt, a, chunk, grid, s), "index kernel"));
+    trace_path("loop_cols nin=%d n_out=%lld n_in=%lld modes=%d+%d nsplit=%lld vec=%d", nin, (long long)n_out,
+               (long long)n_in, outer.n, inner.n, (long long)nsplit, (int)vec);
+    OME_CK(cuda_err(launch_loop_cols(dt, a, chunk, grid, vec, s), "index kernel"));
     if (nsplit > 1) OME_CK(cuda_err(launch_loop_finish(dt, a, s), "index kernel finish"));
     return OME_OK;
   }

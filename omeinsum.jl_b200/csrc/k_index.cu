@@ -180,18 +180,21 @@ __global__ void __launch_bounds__(256) k_loop_thread(const __grid_constant__ Loo
 // the warp), the summed space cut into nsplit ranges (blockIdx.y), each
 // walked by an odometer; split partials go to a.partial[o * nsplit + s] for
 // k_loop_finish.
-template <class A, int NIN>
+template <class A, int NIN, bool VEC>
 __global__ void __launch_bounds__(256) k_loop_cols(const __grid_constant__ LoopArgs a, int64_t chunk) {
   using T = typename A::T;
   constexpr int NI = NIN > 0 ? NIN : MAXIN;
+  constexpr int V = VEC ? (int)(16 / sizeof(T)) : 1;   // consecutive outputs per thread
   const int nin = NIN > 0 ? NIN : a.nin;
   const T sx = scalar_as<T>(a.sx), sy = scalar_as<T>(a.sy);
   griddep_launch_dependents();
   const int64_t split = blockIdx.y;
   const int64_t jb = split * chunk;
   const int64_t je = min(a.n_in, jb + chunk);
-  for (int64_t o = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; o < a.n_out;
-       o += (int64_t)gridDim.x * blockDim.x) {
+  const int64_t ngroups = a.n_out / V;
+  for (int64_t g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; g < ngroups;
+       g += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t o = g * V;
     int64_t off[NI];
     const int64_t yoff = loop_outer_offsets<NIN>(a, o, off);
     int64_t dig[MAXM];
@@ -209,8 +212,10 @@ __global__ void __launch_bounds__(256) k_loop_cols(const __grid_constant__ LoopA
     // U steps at a time: the odometer first records the U offsets, then all
     // their loads are issued, then they are added in order (the sum order is
     // the sequential one)
-    constexpr int U = 8;
-    T acc = A::zero();
+    constexpr int U = VEC ? 4 : 8;
+    T acc[V];
+#pragma unroll
+    for (int v = 0; v < V; ++v) acc[v] = A::zero();
     for (int64_t jj = jb; jj < je; jj += U) {
       int64_t o2[U][NI];
 #pragma unroll
@@ -231,38 +236,75 @@ __global__ void __launch_bounds__(256) k_loop_cols(const __grid_constant__ LoopA
           }
         }
       }
-      T v[U];
+      T val[U][V];
 #pragma unroll
-      for (int u = 0; u < U; ++u) v[u] = jj + u < je ? loop_prod<A, NIN>(a, o2[u]) : A::zero();
+      for (int u = 0; u < U; ++u) {
+        if constexpr (VEC) {
+          if (jj + u >= je) break;
+#pragma unroll
+          for (int i = 0; i < NI; ++i) {
+            if (i >= nin) break;
+            const T* xi = static_cast<const T*>(a.x[i]) + o2[u][i];
+            T w[V];
+            if (a.str[1 + i][0] == 0) {
+              const T c = xi[0];
+#pragma unroll
+              for (int v = 0; v < V; ++v) w[v] = c;
+            } else {
+              const uint4 w4 = __ldg(reinterpret_cast<const uint4*>(xi));
+              memcpy(w, &w4, sizeof(w4));
+            }
+#pragma unroll
+            for (int v = 0; v < V; ++v) val[u][v] = i == 0 ? w[v] : A::mul(val[u][v], w[v]);
+          }
+        } else {
+          val[u][0] = jj + u < je ? loop_prod<A, NIN>(a, o2[u]) : A::zero();
+        }
+      }
 #pragma unroll
       for (int u = 0; u < U; ++u)
-        if (jj + u < je) acc = A::add(acc, v[u]);
+        if (jj + u < je)
+#pragma unroll
+          for (int v = 0; v < V; ++v) acc[v] = A::add(acc[v], val[u][v]);
     }
-    if (a.nsplit == 1) {
-      T* yp = static_cast<T*>(a.y) + yoff;
-      *yp = epilogue<A>(acc, yp, sx, sy, a.sy_zero, a.sx_one);
-    } else {
-      static_cast<T*>(a.partial)[o * a.nsplit + split] = acc;
+#pragma unroll
+    for (int v = 0; v < V; ++v) {
+      if (a.nsplit == 1) {
+        T* yp = static_cast<T*>(a.y) + yoff + v;
+        *yp = epilogue<A>(acc[v], yp, sx, sy, a.sy_zero, a.sx_one);
+      } else {
+        static_cast<T*>(a.partial)[(o + v) * a.nsplit + split] = acc[v];
+      }
     }
   }
 }
 
-template <class A>
-static cudaError_t launch_loop_cols_t(const LoopArgs& a, int64_t chunk, dim3 grid, cudaStream_t s) {
-  KernelTimer kt(s, "k_loop_cols");
+template <class A, bool VEC>
+static void launch_loop_cols_v(const LoopArgs& a, int64_t chunk, dim3 grid, cudaStream_t s) {
   switch (a.nin) {
-    case 1: k_loop_cols<A, 1><<<grid, 256, 0, s>>>(a, chunk); break;
-    case 2: k_loop_cols<A, 2><<<grid, 256, 0, s>>>(a, chunk); break;
-    case 3: k_loop_cols<A, 3><<<grid, 256, 0, s>>>(a, chunk); break;
-    default: k_loop_cols<A, 0><<<grid, 256, 0, s>>>(a, chunk); break;
+    case 1: k_loop_cols<A, 1, VEC><<<grid, 256, 0, s>>>(a, chunk); break;
+    case 2: k_loop_cols<A, 2, VEC><<<grid, 256, 0, s>>>(a, chunk); break;
+    case 3: k_loop_cols<A, 3, VEC><<<grid, 256, 0, s>>>(a, chunk); break;
+    default: k_loop_cols<A, 0, VEC><<<grid, 256, 0, s>>>(a, chunk); break;
+  }
+}
+
+template <class A>
+static cudaError_t launch_loop_cols_t(const LoopArgs& a, int64_t chunk, dim3 grid, bool vec, cudaStream_t s) {
+  KernelTimer kt(s, "k_loop_cols");
+  if constexpr (sizeof(typename A::T) <= 8 && 16 % sizeof(typename A::T) == 0) {
+    if (vec) launch_loop_cols_v<A, true>(a, chunk, grid, s);
+    else launch_loop_cols_v<A, false>(a, chunk, grid, s);
+  } else {
+    launch_loop_cols_v<A, false>(a, chunk, grid, s);
   }
   count_launch();
   return cudaGetLastError();
 }
 
-cudaError_t launch_loop_cols(ome_dtype dt, const LoopArgs& a, int64_t chunk, dim3 grid, cudaStream_t s) {
+cudaError_t launch_loop_cols(ome_dtype dt, const LoopArgs& a, int64_t chunk, dim3 grid, bool vec, cudaStream_t s) {
   cudaError_t e = cudaErrorInvalidValue;
-  OME_DISPATCH(dt, ALG, e = launch_loop_cols_t<ALG>(a, chunk, grid, s));
+  OME_DISPATCH(dt, ALG, e = launch_loop_cols_t<ALG>(a, chunk, grid, vec, s));
   return e;
 }
 

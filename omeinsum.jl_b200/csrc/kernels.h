@@ -35,7 +35,8 @@ cudaError_t launch_loop_finish(ome_dtype dt, const LoopArgs& a, cudaStream_t s);
 cudaError_t launch_map_rows(ome_dtype dt, const LoopArgs& a, int num_sms, cudaStream_t s);
 // Thread per output along y's fastest mode, summed space split over
 // grid.y ranges of chunk (partials for launch_loop_finish when nsplit > 1).
-cudaError_t launch_loop_cols(ome_dtype dt, const LoopArgs& a, int64_t chunk, dim3 grid, cudaStream_t s);
+// vec: V = 16 / element-size consecutive outputs per thread with 16-byte loads.
+cudaError_t launch_loop_cols(ome_dtype dt, const LoopArgs& a, int64_t chunk, dim3 grid, bool vec, cudaStream_t s);
 // One input, first inner mode contiguous, at most one more inner mode: block
 // per (output, row split) with vector loads (vec) over rows of rchunk.
 cudaError_t launch_reduce_contig(ome_dtype dt, const LoopArgs& a, bool vec, int64_t rchunk, int grid,
