@@ -4,8 +4,12 @@
 //    GPU form ext/CUDAExt.jl:60-113).  Also serves Sum (src/unaryrules.jl:30-40),
 //    Tr (:22-26) on a diagonal view, GEMV/dot/outer/Hadamard-shaped binary
 //    rules and the n-ary fallback.
-//  * k_transpose / k_copy: Permutedims via tensorpermute! (src/utils.jl:122-156),
-//    Repeat (src/unaryrules.jl:44-58, stride-0 input modes) and Identity.
+//  * k_transpose / k_map_rows / k_copy: Permutedims via tensorpermute!
+//    (src/utils.jl:122-156), Repeat (src/unaryrules.jl:44-58, stride-0 input
+//    modes) and Identity; k_map_rows also runs contractions without summed
+//    labels (Hadamard and outer products);
+//  * k_reduce_contig / k_reduce_rows / k_loop_cols: Sum and sum-products
+//    whose summed or output modes are contiguous (dot, GEMV, column sums).
 //  * k_scale, k_acc64*: αβ pre-pass and FP64 cross-slice accumulation.
 #include <string.h>
 #include <mutex>
