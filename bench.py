@@ -68,9 +68,13 @@ def case_work(code, ext):
     return flops, 4 * (nin + nout)
 
 
-def make_inputs(code, ext, seed):
+def make_inputs(code, ext, seed, dtype="f32"):
+    """Column-major inputs of a suite contraction: normal(0,1) FP32, or
+    uniform integers in [-8, 8] for Int64."""
     rng = np.random.default_rng(seed)
     ixs, _ = parse_code(code)
+    if dtype == "i64":
+        return [np.asfortranarray(rng.integers(-8, 9, [ext[l] for l in ix], dtype=np.int64)) for ix in ixs]
     return [np.asfortranarray(rng.standard_normal([ext[l] for l in ix]).astype(np.float32)) for ix in ixs]
 
 
@@ -143,14 +147,99 @@ class ClockSampler:
                 "samples": len(sm), "window": "from 1 s of warm-up load through the timed steps"}
 
 
-def cpu_suite(O, inputs, steps=1):
-    """Oracle (NumPy DefaultBackend restatement) on the suite; returns seconds per pass."""
+L2_POLICY = ("GPU arm: L2 flushed before every contraction (outside its events) by a 256 MiB write followed by "
+             "a 256 MiB read, so that no dirty lines remain in L2; CPU arm: inputs of 21 MB to 2 GB per "
+             "contraction, beyond the host caches")
+
+
+def cpu_suite(O, inputs, steps=1, results=None):
+    """Oracle (NumPy DefaultBackend restatement) on the suite; returns seconds
+    per pass (and the last pass's results in `results` when given)."""
     t0 = time.perf_counter()
     for _ in range(steps):
         for (name, code, ext, seed), xs in zip(CASES, inputs):
             ixs, iy = parse_code(code)
-            O.einsum(ixs, iy, xs, ext)
+            r = O.einsum(ixs, iy, xs, ext)
+            if results is not None:
+                results[name] = r
     return (time.perf_counter() - t0) / steps
+
+
+def relerr(got, want):
+    got = np.asarray(got, dtype=np.float64)
+    want = np.asarray(want, dtype=np.float64)
+    n = max(np.linalg.norm(got.ravel()), np.linalg.norm(want.ravel()))
+    d = np.linalg.norm((got - want).ravel())
+    return 0.0 if d == 0 else float(d / max(n, 1e-300))
+
+
+def suite_parity(O, fp32_inputs, fp32_gpu, fp32_oracle, i64_inputs, i64_gpu):
+    """The GPU results of the timed suite against the oracle (the checker):
+    FP32 against the oracle in FP64 and in FP32 (rtol 1e-5 is the reference's
+    GPU agreement tolerance), Int64 entry for entry."""
+    out = {}
+    for (name, code, ext, _), xs in zip(CASES, fp32_inputs):
+        ixs, iy = parse_code(code)
+        w64 = O.einsum(ixs, iy, [x.astype(np.float64) for x in xs], ext)
+        out[name] = {"fp32_rel_err_vs_fp64_oracle": relerr(fp32_gpu[name], w64),
+                     "fp32_rel_err_vs_fp32_oracle": relerr(fp32_gpu[name], fp32_oracle[name])}
+    if i64_gpu:
+        for (name, code, ext, _), xs in zip(CASES, i64_inputs):
+            ixs, iy = parse_code(code)
+            w = O.einsum(ixs, iy, xs, ext)
+            g = i64_gpu[name]
+            out[name]["int64_bit_exact"] = bool(g.dtype == w.dtype and g.shape == w.shape and np.array_equal(g, w))
+    out["all_within_1e-5_and_int64_exact"] = all(
+        v["fp32_rel_err_vs_fp64_oracle"] <= 1e-5 and v.get("int64_bit_exact", True)
+        for k, v in out.items() if isinstance(v, dict))
+    return out
+
+
+def int64_section(ome, dev, steps, flush_l2, lib):
+    """The rule suite in Int64 (uniform integers in [-8, 8], the same seeds):
+    per contraction the event-timed device time with the L2 flushed before it,
+    and the main kernel; results are returned for the exactness check."""
+    import ctypes as C
+    import torch
+    per, kern, inputs, results = {}, {}, [], {}
+    for i, (name, code, ext, seed) in enumerate(CASES):
+        xs = make_inputs(code, ext, seed, "i64")
+        inputs.append(xs)
+        d = [torch.from_numpy(x).to(dev) for x in xs]
+        ixs, iy = parse_code(code)
+        c = ome.EinCode(ixs, iy)
+        y = ome.get_output_array(d, [ext[l] for l in iy])
+        for _ in range(2):
+            ome.einsum_(c, d, y, True, False, ext)
+        torch.cuda.synchronize()
+        lib.ome_kernel_timing(8)
+        ome.einsum_(c, d, y, True, False, ext)
+        torch.cuda.synchronize()
+        fb, nb, cnt = (C.c_float * 8)(), (C.c_char_p * 8)(), C.c_int32()
+        lib.ome_kernel_times(8, fb, nb, C.byref(cnt))
+        lib.ome_kernel_timing(0)
+        kern[name] = "+".join(nb[j].decode() for j in range(cnt.value))
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+        for k in range(steps):
+            flush_l2(k)
+            ev[k][0].record()
+            ome.einsum_(c, d, y, True, False, ext)
+            ev[k][1].record()
+        torch.cuda.synchronize()
+        ome.device_status()
+        per[name] = sum(a.elapsed_time(b) for a, b in ev) / steps
+        results[name] = y.cpu().numpy()
+        del d, y
+    step_ms = sum(per.values())
+    detail = {}
+    for name, code, ext, _ in CASES:
+        f, b = case_work(code, ext)
+        detail[name] = {"us": per[name] * 1e3, "main_kernel": kern[name], "GB/s": 2 * b / (per[name] / 1e3) / 1e9}
+        if f:
+            detail[name]["Gop/s"] = f / (per[name] / 1e3) / 1e9
+    return {"workload": WORKLOAD.replace("FP32", "Int64") + "; uniform integers in [-8, 8]",
+            "contractions_per_s": len(CASES) / (step_ms / 1e3), "ms_per_step": step_ms, "steps": steps,
+            "per_case": detail}, inputs, results
 
 
 def run_case_only(ome, name, dev):
@@ -394,7 +483,8 @@ def run_reference(args, rank):
     line = {"metric": METRIC, "value": v, "unit": "contractions/s", "n_gpus": args.gpus, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": t * 1e3, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded normal(0,1))",
-            "config": {"workload": WORKLOAD}, "impl": "reference",
+            "config": {"workload": WORKLOAD, "l2": L2_POLICY}, "impl": "reference",
+            "prec": "plain FP32 (OpenBLAS SGEMM on the host cores)", "parallelism": "rank 0 only",
             "cpu_baseline": {"value": v, "unit": "contractions/s", "cores": cores, "kind": "port",
                              "sample": f"the full suite, {args.steps} passes, NumPy/OpenBLAS DefaultBackend "
                                        f"restatement (OPENBLAS threads = {cores}; copies single-threaded)"},
@@ -413,6 +503,7 @@ def main():
     ap.add_argument("--no-tn", action="store_true", help="skip the tensor-network precision section")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched MPS-transfer section")
     ap.add_argument("--no-serve", action="store_true", help="skip the serving section")
+    ap.add_argument("--no-int64", action="store_true", help="skip the Int64 rule-suite section")
     ap.add_argument("--tn-sharded", action="store_true",
                     help="run the slice-sharded network section at N=1 too (a one-rank NCCL group)")
     ap.add_argument("--case", default=None,
@@ -595,15 +686,22 @@ def main():
                 "kernel_us": dur_s * 1e6, "case_us": case_s * 1e6, "case_frac": (nbytes / case_s / 1e9) / hbm,
                 "peak_source": f"{src} hbm_gbs"}
 
-    cpu = None
+    i64 = i64_inputs = i64_results = None
+    if not args.no_int64:
+        i64, i64_inputs, i64_results = int64_section(ome, dev, args.steps, flush_l2, lib)
+
+    cpu = parity = None
     if rank == 0 and world == 1 and not args.no_cpu:
         sys.path.insert(0, os.path.join(ROOT, "oracle"))
         import ome_oracle as O
         inputs = [[h.numpy() for h in hs] for hs in hosts]
-        tc = cpu_suite(O, inputs, 1)
+        oracle_out = {}
+        tc = cpu_suite(O, inputs, 1, oracle_out)
         cpu = {"value": len(CASES) / tc, "unit": "contractions/s", "cores": os.cpu_count(), "kind": "port",
                "sample": "the full suite once, NumPy/OpenBLAS DefaultBackend restatement "
                          f"(BLAS threads = {os.cpu_count()}; copies single-threaded)"}
+        gpu_out = {name: o.cpu().numpy() for (name, _, _, _), o in zip(CASES, outs)}
+        parity = suite_parity(O, inputs, gpu_out, oracle_out, i64_inputs, i64_results)
 
     del devs, outs, flush, clean
     ome.release_workspaces()
@@ -627,13 +725,12 @@ def main():
         line = {"metric": METRIC, "value": value, "unit": "contractions/s", "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "warmup_steps_run": nw, "ms_per_step": step_ms_max, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded normal(0,1))",
-                "config": {"workload": WORKLOAD,
-                           "l2": "flushed before every contraction (outside its events) by a 256 MiB write "
-                                 "followed by a 256 MiB read, so that no dirty lines remain in L2",
-                           "prec": {0: "BF16x6 tensor-core split products (FP32-faithful) where GEMM-shaped",
-                                    1: "plain FP32 (CUDA cores)", 2: "BF16x3 where GEMM-shaped",
-                                    3: "BF16x6 where GEMM-shaped"}[args.prec],
-                           "parallelism": f"replicas x{world}", "per_case": detail},
+                "config": {"workload": WORKLOAD, "l2": L2_POLICY},
+                "prec": {0: "BF16x6 tensor-core split products (FP32-faithful) where GEMM-shaped",
+                         1: "plain FP32 (CUDA cores)", 2: "BF16x3 where GEMM-shaped",
+                         3: "BF16x6 where GEMM-shaped"}[args.prec],
+                "parallelism": f"replicas x{world}", "per_case": detail, "parity_vs_oracle": parity,
+                "int64_suite": i64,
                 "e2e": {"value": e2e_value, "unit": "contractions/s", "h2d_bytes_per_step": h2d,
                         "d2h_bytes_per_step": d2h, "api": "einsum_many", "serial_einsum_value": e2e_serial},
                 "gpu_launches": int(launches), "roofline": roof, "cpu_baseline": cpu,

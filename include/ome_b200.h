@@ -156,6 +156,16 @@ OME_API int ome_loop_einsum(ome_ctx* ctx, void* stream, ome_dtype dtype, int32_t
                     const ome_tensor* xs, const ome_tensor* y, const void* sx,
                     const void* sy);
 
+/* einsum_grad(ixs, xs, iy, size_dict, dy, i) (src/autodiff.jl:24-30): the
+ * gradient of einsum(ixs -> iy)(xs) with respect to input i (0-based):
+ * dx <- conj(einsum((ixs with iy in place of ixs[i]) -> ixs[i])(xs with
+ * conj(dy) in place of xs[i])).  dy carries iy as its labels; dx must have
+ * xs[i]'s labels and extents (xs[i].data is not read and may be NULL).
+ * Replaces the per-input pullback of rrule(einsum) (src/autodiff.jl:35-44). */
+OME_API int ome_einsum_grad(ome_ctx* ctx, void* stream, ome_dtype dtype, int32_t ninputs,
+                            const ome_tensor* xs, const ome_tensor* dy, int32_t i,
+                            const ome_tensor* dx, int32_t prec);
+
 /* Contraction trees (NestedEinsum / SlicedEinsum) -------------------------- */
 
 /* A tree is given in post-order, root last.  Node j has node_nargs[j]

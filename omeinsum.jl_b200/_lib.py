@@ -22,7 +22,7 @@ PREC_AUTO, PREC_FP32, PREC_BF16X3, PREC_BF16X6 = range(4)
 EXPORTS = [
     "ome_version", "ome_launch_count", "ome_device_status", "ome_selftest_wait_timeout",
     "ome_kernel_timing", "ome_kernel_times", "ome_last_error", "ome_ctx_create", "ome_ctx_destroy", "ome_ctx_workspace_bytes",
-    "ome_einsum", "ome_loop_einsum", "ome_plan_create", "ome_plan_destroy", "ome_plan_peak_bytes",
+    "ome_einsum", "ome_loop_einsum", "ome_einsum_grad", "ome_plan_create", "ome_plan_destroy", "ome_plan_peak_bytes",
     "ome_plan_execute", "ome_plan_gradient", "ome_plan_slice_count", "ome_plan_partial_info",
     "ome_plan_execute_slices", "ome_plan_finish", "ome_reduce_noalloc", "ome_batch_create", "ome_batch_run",
     "ome_batch_info", "ome_batch_destroy", "ome_treesa", "ome_greedy", "ome_slice_greedy",
@@ -84,6 +84,8 @@ def load() -> C.CDLL:
         lib.ome_ctx_workspace_bytes.argtypes = [P, C.POINTER(C.c_size_t)]
         lib.ome_einsum.argtypes = [P, P, C.c_int, C.c_int32, C.POINTER(Tensor), C.POINTER(Tensor), P, P, C.c_int32]
         lib.ome_loop_einsum.argtypes = [P, P, C.c_int, C.c_int32, C.POINTER(Tensor), C.POINTER(Tensor), P, P]
+        lib.ome_einsum_grad.argtypes = [P, P, C.c_int, C.c_int32, C.POINTER(Tensor), C.POINTER(Tensor), C.c_int32,
+                                        C.POINTER(Tensor), C.c_int32]
         lib.ome_plan_create.argtypes = [P, C.c_int, C.c_int32, i32p, i32p, C.c_int32, i32p, i32p, i32p, i32p,
                                         C.c_int32, i32p, i64p, C.c_int32, i32p, C.c_int32, C.POINTER(P)]
         lib.ome_plan_destroy.argtypes = [P]

@@ -891,4 +891,72 @@ int ome_loop_einsum(ome_ctx* ctx, void* stream, ome_dtype dtype, int32_t ninputs
   return einsum_entry(ctx, stream, dtype, ninputs, xs, y, sx, sy, OME_PREC_FP32, true);
 }
 
+// einsum_grad (src/autodiff.jl:24-30): dx <- conj(einsum(ixs with iy in place
+// of ixs[i] -> ixs[i])(xs with conj(dy) in place of xs[i])).  For complex
+// dtypes conj(dy) goes to a column-major workspace copy and the result is
+// conjugated in place (through a workspace copy when dx is strided).
+int ome_einsum_grad(ome_ctx* ctx, void* stream, ome_dtype dtype, int32_t ninputs, const ome_tensor* xs,
+                    const ome_tensor* dy, int32_t i, const ome_tensor* dx, int32_t prec) {
+  if (!ctx || !xs || !dy || !dx) return set_err(OME_INVALID_ARGUMENT, "NULL argument");
+  if ((int)dtype < 0 || (int)dtype > OME_TROP_F64) return set_err(OME_INVALID_ARGUMENT, "unknown dtype %d", (int)dtype);
+  if (ninputs < 1) return set_err(OME_INVALID_ARGUMENT, "number of input tensors must be greater than 0");
+  if (ninputs > MAXIN) return set_err(OME_UNSUPPORTED, "at most %d input tensors per contraction", MAXIN);
+  if (i < 0 || i >= ninputs) return set_err(OME_INVALID_ARGUMENT, "input index %d outside [0, %d)", i, ninputs);
+  if (xs[i].ndim != dx->ndim) return set_err(OME_INVALID_ARGUMENT, "the gradient must have the rank of input %d", i);
+  for (int d = 0; d < dx->ndim; ++d) {
+    if (!xs[i].labels || !dx->labels || xs[i].labels[d] != dx->labels[d])
+      return set_err(OME_INVALID_ARGUMENT, "the gradient's labels must be those of input %d", i);
+    if (xs[i].dims && xs[i].dims[d] != dx->dims[d])
+      return set_err(OME_DIMENSION_MISMATCH, "label %d = %lld or %lld)?", dx->labels[d],
+                     (long long)xs[i].dims[d], (long long)dx->dims[d]);
+  }
+  HView xv[MAXIN], dyv, dxv;
+  for (int k = 0; k < ninputs; ++k)
+    if (k != i) OME_CK(view_from_tensor(xs[k], xv[k], "input"));
+  OME_CK(view_from_tensor(*dy, dyv, "cotangent"));
+  OME_CK(view_from_tensor(*dx, dxv, "gradient"));
+  ctx->ws_top = 0;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  const Scalar one = scalar_one(dtype), zero = scalar_zero(dtype);
+  const bool cplx = dtype == OME_C32 || dtype == OME_C64;
+  const size_t es = dtype_size(dtype);
+  auto contiguous_copy = [&](const HView& v, HView& c) -> int {
+    c = v;
+    int64_t st = 1;
+    for (int d = 0; d < v.nd; ++d) {
+      c.str[d] = st;
+      st *= v.ext[d];
+    }
+    c.data = static_cast<char*>(ws_alloc(ctx, (size_t)std::max<int64_t>(st, 1) * es));
+    if (!c.data) return set_err(OME_OUT_OF_MEMORY, "workspace too small for a gradient temporary (%lld elements)",
+                                (long long)st);
+    return OME_OK;
+  };
+  if (cplx) {
+    HView c;
+    OME_CK(contiguous_copy(dyv, c));
+    OME_CK(einsum_views(ctx, s, dtype, 1, &dyv, c, one, zero, prec, false));
+    OME_CK(cuda_err(launch_conj(dtype, c.data, std::max<int64_t>(numel(c), 1), s), "conj"));
+    xv[i] = c;
+  } else {
+    xv[i] = dyv;
+  }
+  bool dense = true;
+  {
+    int64_t st = 1;
+    for (int d = 0; d < dxv.nd; ++d) {
+      if (dxv.ext[d] > 1 && dxv.str[d] != st) dense = false;
+      st *= dxv.ext[d];
+    }
+  }
+  HView out = dxv;
+  if (cplx && !dense) OME_CK(contiguous_copy(dxv, out));
+  OME_CK(einsum_views(ctx, s, dtype, ninputs, xv, out, one, zero, prec, false));
+  if (cplx) {
+    OME_CK(cuda_err(launch_conj(dtype, out.data, std::max<int64_t>(numel(out), 1), s), "conj"));
+    if (!dense) OME_CK(einsum_views(ctx, s, dtype, 1, &out, dxv, one, zero, prec, false));
+  }
+  return OME_OK;
+}
+
 }  // extern "C"

@@ -13,7 +13,10 @@
 // keeps it until the process exits.  In host code the array's name is only a
 // host-side stand-in: the device address is looked up once per device with
 // cudaGetSymbolAddress, with that device current, by the first call made on
-// that device (make that first call before any stream capture).  All calls
+// that device (make that first call before any stream capture).  The address
+// is cached for the life of the process: after cudaDeviceReset the library's
+// module is loaded again at another address, so this entry point must not be
+// used across a cudaDeviceReset of a device it has already run on.  All calls
 // on a device share the array and it keeps the last call's contents; the
 // first pass overwrites every partial the second pass reads, so nothing has
 // to be cleared, but calls that overlap on the GPU (several streams, or
@@ -79,8 +82,8 @@ extern "C" int ome_reduce_noalloc(void* stream, ome_dtype dtype, const ome_tenso
     const int k = find(xu, yu.lab[d]);
     if (k < 0) return set_err(OME_INVALID_ARGUMENT, "output label %d is not an input label", yu.lab[d]);
     if (xu.ext[k] != yu.ext[d])
-      return set_err(OME_DIMENSION_MISMATCH, "label %d = %lld or %lld)?", yu.lab[d], (long long)xu.ext[k],
-                     (long long)yu.ext[d]);
+      return set_err(OME_DIMENSION_MISMATCH, "label %d: input extent %lld, output extent %lld", yu.lab[d],
+                     (long long)xu.ext[k], (long long)yu.ext[d]);
   }
   int dev = 0;
   cudaError_t ce = cudaGetDevice(&dev);
@@ -116,6 +119,14 @@ extern "C" int ome_reduce_noalloc(void* stream, ome_dtype dtype, const ome_tenso
     ++ni;
   }
   if (n_out == 0) return OME_OK;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  if (n_in == 0) {
+    // a summed label of extent 0: the sum is the algebra's zero, so
+    // y <- sy*y (zero when sy is zero); no partial sums are needed
+    const Scalar sy = scalar_from(dtype, syp);
+    return cuda_err(launch_scale(dtype, yu.data, yu.nd, yu.ext, yu.str, sy, scalar_is_zero(dtype, sy) ? 1 : 0, sms, s),
+                    "no-alloc reduction (empty sum)");
+  }
   const size_t es = dtype_size(dtype);
   const size_t cap = OME_NOALLOC_SCRATCH_BYTES;
   if ((size_t)n_out * 2 * es > cap)
@@ -151,7 +162,6 @@ extern "C" int ome_reduce_noalloc(void* stream, ome_dtype dtype, const ome_tenso
       step /= a.ext[no + m];
     }
   }
-  cudaStream_t s = static_cast<cudaStream_t>(stream);
   const int grid = (int)std::min<int64_t>(n_out * nsplit, (int64_t)sms * 32);
   rc = cuda_err(launch_loop(dtype, a, LOOP_BLOCK, grid, block, s), "no-alloc reduction");
   if (rc) return rc;

@@ -418,21 +418,48 @@ def loop_einsum_(ixs, iy, xs, y, sx, sy, size_dict=None):
 def einsum_grad(ixs, xs, iy, size_dict, dy, i):
     """``einsum_grad`` (src/autodiff.jl:24-30): the gradient of ``einsum`` w.r.t.
     input ``i`` (0-based): contract conj(dy) in place of input i into ixs[i],
-    then conjugate."""
-    nixs = [tuple(ix) for ix in ixs]
-    nixs[i] = tuple(iy)
-    nxs = list(xs)
-    dyt = _as_tensor(dy)
-    if isinstance(dyt, torch.Tensor) and dyt.is_complex():
-        dyt = torch.conj_physical(dyt)
-    nxs[i] = dyt
-    y = einsum(EinCode(nixs, ixs[i]), nxs, size_dict)
-    if isinstance(y, torch.Tensor) and y.is_complex():
-        y = torch.conj_physical(y)
-        xi = _as_tensor(xs[i])
-        if isinstance(xi, torch.Tensor) and not xi.is_complex():
-            y = y.real.contiguous()
-    return y
+    then conjugate -- one ``ome_einsum_grad`` call (the conjugations run in
+    the library).  A real input of a complex contraction gets the real part
+    (``ProjectTo(xs[i])``)."""
+    be = _require_b200()
+    ixs = [tuple(ix) for ix in ixs]
+    nxs = [_as_tensor(x) for x in xs]
+    nxs[i] = _as_tensor(dy)
+    p = _Prepared(nxs)
+    ts = p.tensors
+    lm = _LabelMap()
+    keep: list = []
+    structs = (_lib.Tensor * len(ixs))()
+    for k, (ix, t) in enumerate(zip(ixs, ts)):
+        if k == i:
+            continue
+        if len(ix) != t.dim():
+            raise ArgumentError(f"indices {ix} invalid for tensor with ndims = {t.dim()}")
+        structs[k] = _tensor_struct(t, [lm(l) for l in ix], keep)
+    if len(tuple(iy)) != ts[i].dim():
+        raise ArgumentError(f"indices {tuple(iy)} invalid for the cotangent with ndims = {ts[i].dim()}")
+    dyt = _tensor_struct(ts[i], [lm(l) for l in iy], keep)
+    if size_dict is None:
+        size_dict = get_size_dict([ix for k, ix in enumerate(ixs) if k != i] + [tuple(iy)],
+                                  [t for k, t in enumerate(ts) if k != i] + [ts[i]])
+    shape = [size_dict[l] for l in ixs[i]]
+    out = _alloc(shape, p.dtype, p.device)
+    dxt = _tensor_struct(out, [lm(l) for l in ixs[i]], keep)
+    nd = len(shape)
+    dims = (C.c_int64 * max(nd, 1))(*shape)
+    labs = (C.c_int32 * max(nd, 1))(*[lm(l) for l in ixs[i]])
+    keep.extend([dims, labs])
+    structs[i] = _lib.Tensor(None, nd, dims, None, labs)
+    dev = out.device.index
+    ctx = _lib.context(dev)
+    with torch.cuda.device(dev):
+        check(_lib.load().ome_einsum_grad(ctx.handle, _stream(dev), p.ome, len(ixs), structs, C.byref(dyt), i,
+                                          C.byref(dxt), be.prec))
+    xi = _as_tensor(xs[i])
+    xi = xi.data if isinstance(xi, TropicalTensor) else xi
+    if out.is_complex() and not xi.is_complex():
+        out = out.real.contiguous()
+    return p.wrap(out)
 
 
 def cost_and_gradient(code, xs, dy=None):

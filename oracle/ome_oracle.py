@@ -67,7 +67,18 @@ class Algebra:
             return np.sum(x, axis=tuple(axes), dtype=x.dtype)
 
     def matmul(self, a, b):
-        """Batched (..., m, k) @ (..., k, n) in the working dtype (BLAS for floats)."""
+        """Batched (..., m, k) @ (..., k, n) in the working dtype (BLAS for floats).
+
+        Int64 (Julia's generic ``mul!``, ``src/binaryrules.jl:129-131``):
+        when max|a| * max|b| * k < 2^53 every partial sum is an integer that
+        FP64 holds exactly and no Int64 wrap-around can occur, so the product
+        is formed by FP64 BLAS and converted back -- the same integers as the
+        Int64 loop, in a fraction of the time.  Otherwise NumPy's Int64
+        matmul (wrapping, like Julia's Int64)."""
+        if a.dtype == np.int64 and b.dtype == np.int64 and a.size and b.size:
+            bound = float(np.max(np.abs(a))) * float(np.max(np.abs(b))) * a.shape[-1]
+            if bound < 2.0 ** 53:
+                return np.matmul(a.astype(np.float64), b.astype(np.float64)).astype(np.int64)
         with np.errstate(over="ignore"):
             return np.matmul(a, b)
 

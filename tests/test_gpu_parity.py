@@ -353,3 +353,29 @@ def test_batch_innermost_gemm(code, sizes, dt):
         yd = to_dev(y0, dt)
         ome.einsum_(c, [to_dev(x, dt) for x in xs], yd, 3, 2, sizes)
         assert_match(to_np(yd), 3 * oracle(ixs, iy, xs, sizes, dt) + 2 * y0, dt)
+
+
+@pytest.mark.parametrize("dts,want_dtype", [
+    (("i64", "f32"), torch.float32),       # Julia: promote_type(Int64, Float32) == Float32 (NumPy would give float64)
+    (("bool", "i64"), torch.int64),
+    (("f32", "f64"), torch.float64),
+    (("i64", "c64"), torch.complex64),
+    (("f32", "c128"), torch.complex128),
+])
+@pytest.mark.parametrize("code", ["ij,jk->ik", "ij,jk,kl->il", "ijk,jkl->il"])
+def test_mixed_eltype_inputs(code, dts, want_dtype):
+    """Mixed-eltype inputs: the output eltype is Julia's promote_type of the
+    inputs' (src/loop_einsum.jl:55-61, ext/CUDAExt.jl:34-47) and the inputs are
+    converted to it before contracting (ext/CUDAExt.jl:116)."""
+    rng = np.random.default_rng(21)
+    ixs, iy = parse(code)
+    sd = {l: 5 + (ord(l) % 4) for l in "ijkl"}
+    kinds = [dts[k % 2] for k in range(len(ixs))]
+    xs = [gen(rng, [sd[l] for l in ix], dt) for ix, dt in zip(ixs, kinds)]
+    got = ome.einsum(ome.EinCode(ixs, iy), [to_dev(x, dt) for x, dt in zip(xs, kinds)], sd)
+    assert got.dtype == want_dtype
+    want = O.einsum(ixs, iy, xs, sd)
+    assert str(want.dtype) == str(want_dtype).replace("torch.", "")
+    tgt = {torch.float32: "f32", torch.float64: "f64", torch.int64: "i64", torch.complex64: "c64",
+           torch.complex128: "c128"}[want_dtype]
+    assert_match(to_np(got), want, tgt)

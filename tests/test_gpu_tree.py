@@ -149,3 +149,40 @@ def test_sliced_network_many_nodes(dt):
     assert_match(got, want, dt, 1e-5 if dt == "f32" else None)
     got2 = to_np(opt(*[to_dev(x, dt) for x in xs]))
     assert_match(got2, want, dt, 1e-5 if dt == "f32" else None)
+
+
+def test_config3_network_slices_against_oracle():
+    """The precision benchmark's network (random 3-regular graph, n = 180,
+    bond 2, FP32 normal(0,1)/sqrt(3), greedy order, sliced to 2^27 elements):
+    the device's FP64 partial over the first and the last slice against the
+    oracle's restatement of the slice loop (src/slicing.jl:118-137) on the
+    same slices in FP64, and the BF16x6 FP32 partials against the same FP64
+    oracle at 1e-5.  This anchors the benchmark's "error vs FP64" figures,
+    which compare the device's own runs, to an independent evaluation."""
+    import os
+    import sys
+    sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+    import bench
+    code, sd, xs = bench.tn_network(ome, 180)
+    opt = ome.optimize_code(code, sd, ome.GreedyMethod(nrepeat=10, seed=0))
+    se = ome.slice_code(opt, sd, ome.GreedySlicer(sc_target=27))
+    tree = oracle_tree(se.eins)
+    x64 = [x.astype(np.float64) for x in xs]
+    ome.set_einsum_backend(ome.B200Backend(prec=3))
+    try:
+        sh64 = ome.ShardedSlices(se, [torch.from_numpy(x).cuda() for x in x64])
+        sh32 = ome.ShardedSlices(se, [torch.from_numpy(x).cuda() for x in xs])
+        n = sh64.nslices
+        assert n >= 2
+        for b in (0, n - 1):
+            want = O.sliced_partial(list(se.slicing), tree, x64, sd, b, b + 1)
+            sh64.range = (b, b + 1)
+            got64 = to_np(sh64.partial([torch.from_numpy(x).cuda() for x in x64]))
+            ome.device_status()
+            assert relerr(got64, want) <= 1e-12, (b, relerr(got64, want))
+            sh32.range = (b, b + 1)
+            got32 = to_np(sh32.partial([torch.from_numpy(x).cuda() for x in xs]))
+            ome.device_status()
+            assert relerr(got32, want) <= 1e-5, (b, relerr(got32, want))
+    finally:
+        ome.set_einsum_backend(ome.B200Backend())

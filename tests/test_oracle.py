@@ -395,3 +395,17 @@ def test_bool_and_int_semantics():
     big = np.array([2 ** 62, 2 ** 62], dtype=np.int64)
     r = O.einsum([("i",), ("i",)], (), [big, np.array([2, 2], dtype=np.int64)])
     assert r[()] == np.int64(0)  # 2^64 wraps to 0 like Julia Int64
+
+
+def test_int64_matmul_exact_path_equals_integer_loop():
+    """The oracle's Int64 GEMM (FP64 BLAS when every partial sum is an integer
+    below 2^53) gives the same integers as NumPy's Int64 matmul, and large
+    values still wrap like Julia's Int64."""
+    rng = np.random.default_rng(1)
+    a = rng.integers(-8, 9, (3, 40, 70), dtype=np.int64)
+    b = rng.integers(-8, 9, (3, 70, 30), dtype=np.int64)
+    got = O.REAL.matmul(a, b)
+    assert got.dtype == np.int64 and np.array_equal(got, np.matmul(a, b))
+    big = np.full((2, 2), 2 ** 62, dtype=np.int64)
+    with np.errstate(over="ignore"):
+        assert np.array_equal(O.REAL.matmul(big, big), np.matmul(big, big))
