@@ -540,22 +540,27 @@ static int reduce_dangling(ome_ctx* ctx, cudaStream_t s, ome_dtype dt, HView& xu
   return OME_OK;
 }
 
-// Tensor-core kernel for an FP32 GEMM: 1 = pre-split operands + bulk-copy
-// persistent kernel (k_gemm_packed), 0 = in-kernel converters
-// (k_gemm_bf16x3).  The environment variable OME_GEMM=packed|fused overrides
-// the shape rule.
+// Tensor-core kernel for an FP32 GEMM: 2 = the 2-SM kernel fed by tensor
+// maps over the FP32 operands (k_gemm_tma2), 1 = pre-split operands +
+// bulk-copy persistent kernel (k_gemm_packed), 0 = in-kernel converters
+// (k_gemm_bf16x3).  The environment variable OME_GEMM=tma|packed|fused
+// overrides the shape rule (a kernel whose preconditions fail falls through
+// to the next).
 static int gemm_kernel_choice(const GemmArgs& g) {
   static const int forced = [] {
     const char* e = getenv("OME_GEMM");
     if (!e) return -1;
+    if (!strcmp(e, "tma")) return 2;
     if (!strcmp(e, "packed")) return 1;
     if (!strcmp(e, "fused")) return 0;
     return -1;
   }();
   if (forced >= 0) return forced;
+  const double flops = 2.0 * (double)g.M * (double)g.N * (double)g.K * (double)g.L;
+  // 256 x 256 cluster tiles: worth it once a few waves of k-steps are there
+  if (gemm_tma2_applies(g) && g.M >= 128 && g.N >= 128 && g.K >= 256 && flops >= 2e8) return 2;
   // pre-splitting pays for itself on large GEMMs with a long K only (two
   // extra HBM passes over the operands; with a short K the output dominates)
-  const double flops = 2.0 * (double)g.M * (double)g.N * (double)g.K * (double)g.L;
   return g.M >= 256 && g.N >= 256 && g.K >= 512 && flops >= 1e9 ? 1 : 0;
 }
 
@@ -685,7 +690,16 @@ static int run_binary(ome_ctx* ctx, cudaStream_t s, ome_dtype dt, HView x1, HVie
       size_t avail = ctx->ws_bytes > ctx->ws_top ? ctx->ws_bytes - ((ctx->ws_top + 255) & ~(size_t)255) : 0;
       void* w = avail ? ctx->ws + ((ctx->ws_top + 255) & ~(size_t)255) : nullptr;
       const int nterms = prec == OME_PREC_BF16X3 ? 2 : 3;
-      if (gemm_kernel_choice(g) == 1) {
+      const int choice = gemm_kernel_choice(g);
+      if (choice == 2) {
+        cudaError_t e = launch_gemm_tma2(g, nterms, w, avail, ctx->num_sms, s);
+        if (e != cudaErrorNotSupported) {
+          trace_path("  -> tma2");
+          return cuda_err(e, "tma bf16 split gemm");
+        }
+        cudaGetLastError();
+      }
+      if (choice >= 1) {
         void* pw = w;
         size_t pavail = avail;
         const size_t need = gemm_packed_bytes(g, nterms, ctx->num_sms);

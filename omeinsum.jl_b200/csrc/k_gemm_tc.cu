@@ -28,8 +28,10 @@
 //    sums in a fixed order (deterministic);
 //  * every mbarrier wait is bounded (about 2 s of %globaltimer); on expiry the
 //    kernel records g_ome_timeout, stops waiting and frees its TMEM.
+#include <cuda.h>
 #include <cuda_bf16.h>
 #include <string.h>
+#include <mutex>
 #include "kernels.h"
 
 namespace ome {
@@ -1022,6 +1024,749 @@ cudaError_t launch_gemm_packed(const GemmArgs& g, int nterms, void* workspace, s
   const int64_t total = Rt * BM * BN;
   const int64_t nb = (total + 255) / 256;
   k_splitk_tiles<<<(unsigned)std::min<int64_t>(nb, (int64_t)num_sms * 16), 256, 0, s>>>(t);
+  count_launch();
+  return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// k_gemm_tma2: 2-SM tensor-core GEMM fed by tensor maps over the FP32 inputs.
+//
+// The operands are read in place, through TMA tensor maps whose dimensions
+// and strides are the contraction's merged mode groups (the permutation of
+// simplifyto, src/einsum.jl:127-134, lives in the maps: nothing is written
+// back to HBM), and split into BF16 terms in shared memory.
+//  * A cluster of two CTAs computes a 256 x 256 tile of C with
+//    tcgen05.mma.cta_group::2 (M = 256, N = 256, K = 16): CTA r holds rows
+//    128r..128r+127 of the A tile and columns 128r..128r+127 of the B tile;
+//    its TMEM receives rows 128r.. of the accumulator, all 256 columns.
+//  * Warp 16 (one thread) issues, per 32-wide k stage, the TMA loads of this
+//    CTA's FP32 A and B tiles (128-byte swizzle, zero fill past the extents;
+//    no multicast) into one of three FP32 stages.
+//  * Warps 0-7 (A) and 8-15 (B) convert a stage into NT BF16 terms per value
+//    in the UMMA K-major canonical layout (conflict-free shared-memory reads
+//    and writes in both operand orientations), then arrive on the leader
+//    CTA's term_full barrier (remote arrive, release at cluster scope).
+//  * Warp 17 of the leader CTA issues the MMAs (main t0*t0 and cross-term
+//    accumulators, 2 x 256 TMEM columns) and releases each term stage to both
+//    CTAs with a multicast tcgen05.commit.
+//  * Every CHS stages the 16 converter warps of both CTAs drain the
+//    accumulators (tcgen05.ld) into FP32 running sums in registers with
+//    round-to-nearest adds; the accumulators are single-buffered, so the
+//    converters drain chunk c before they wait for a term stage whose MMAs
+//    come after it (no cycle in the waits).
+//  * Persistent over units: whole 256 x 256 tiles for the complete waves of
+//    clusters, the last wave's tiles cut along K (partials summed in split
+//    order by k_splitk_tiles2: deterministic).
+//  * Every wait is bounded (tc::WAIT_NS); on expiry the CTA records the
+//    timeout flag, stops waiting, lets its own copies and MMAs finish and
+//    frees its TMEM.  Both CTAs meet at a final cluster barrier.
+namespace t2 {
+constexpr int BM = 128;                    // rows per CTA (256 per cluster tile)
+constexpr int BK = 32;                     // k per stage
+constexpr int CHS = 8;                     // stages per accumulator chunk (16 k-steps)
+constexpr int F32_STAGES = 2;
+constexpr int NSR = 32;                    // running sums per thread in registers (the other 32 in shared memory)
+constexpr int F32_TILE = BM * BK * 4;      // 16 KB: one operand, one stage
+constexpr int TERM_TILE = BM * BK * 2;     // 8 KB: one term of one operand
+constexpr int NCONV = 512;                 // converter + drain warps 0-15
+constexpr int NTHREADS = NCONV + 64;       // + TMA warp 16 + MMA warp 17
+constexpr int TMEM_COLS = 512;
+template <int NT> struct Cfg {
+  static constexpr int F32_STAGE = 2 * F32_TILE;          // A tile, B tile
+  static constexpr int TERM_STAGE = 2 * NT * TERM_TILE;   // A terms, B terms
+  static constexpr int TSTAGES = NT == 2 ? 3 : 2;
+  static constexpr int SUM_BYTES = NCONV * (64 - NSR) * 4;   // 64 KB of running sums
+  static constexpr int BAR_BYTES = 256;
+  static constexpr int SMEM_BYTES = F32_STAGES * F32_STAGE + TSTAGES * TERM_STAGE + SUM_BYTES + BAR_BYTES + 1024;
+};
+// kind::f16, BF16 x BF16 -> F32, K-major A and B, M = 256 (cta pair), N = 256
+constexpr uint32_t IDESC = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(256 >> 3) << 17) |
+                           ((uint32_t)(256 >> 4) << 24);
+}  // namespace t2
+
+struct T2Args {
+  GemmArgs g;
+  float* partial;                  // [(tiles - F) * S][256][256]
+  int TM, TN, NKT, tiles, F, ksplit, units, S;   // all below 2^31 (checked on the host)
+};
+
+__device__ __forceinline__ uint32_t cluster_rank() {
+  uint32_t r;
+  asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+  return r;
+}
+__device__ __forceinline__ void cluster_sync_all() {
+  asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+// Address of the same shared-memory location in CTA `rank` of the cluster.
+__device__ __forceinline__ uint32_t peer_addr(uint32_t a, uint32_t rank) {
+  uint32_t r;
+  asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(a), "r"(rank));
+  return r;
+}
+// Arrive on an mbarrier of either CTA of the pair (default release at CTA
+// scope: the data it publishes is this CTA's own shared memory, made visible
+// to the tensor core by fence.proxy.async before the arrive; a cluster-scope
+// release would cost a full fence per arrive).
+__device__ __forceinline__ void mbar_arrive_remote(uint32_t cluster_addr) {
+  asm volatile("mbarrier.arrive.shared::cluster.b64 _, [%0];" ::"r"(cluster_addr) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait_cl(uint64_t* bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}\n"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// Bounded wait on a barrier that both CTAs of the pair arrive on.
+__device__ __forceinline__ bool mbar_wait_cl(uint64_t* bar, uint32_t parity, volatile int* abort_flag) {
+  if (mbar_try_wait_cl(bar, parity)) return true;
+  const uint64_t t0 = gtimer();
+  while (true) {
+#pragma unroll 1
+    for (int i = 0; i < 32; ++i)
+      if (mbar_try_wait_cl(bar, parity)) return true;
+    if (*abort_flag) return false;
+    if (gtimer() - t0 > tc::WAIT_NS) {
+      *abort_flag = 1;
+      atomicExch(&g_ome_timeout, 1);
+      return false;
+    }
+  }
+}
+// 32-bit shared-address forms (fewer registers than generic pointers).
+__device__ __forceinline__ bool mbar_try_wait32(uint32_t a, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}\n"
+      : "=r"(ok)
+      : "r"(a), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+__device__ __forceinline__ int ld_flag(uint32_t a) {
+  int v;
+  asm volatile("ld.volatile.shared.u32 %0, [%1];" : "=r"(v) : "r"(a) : "memory");
+  return v;
+}
+__device__ __forceinline__ bool mbar_wait32(uint32_t a, uint32_t parity, uint32_t abort_a) {
+  if (mbar_try_wait32(a, parity)) return true;
+  const uint64_t t0 = gtimer();
+  while (true) {
+#pragma unroll 1
+    for (int i = 0; i < 32; ++i)
+      if (mbar_try_wait32(a, parity)) return true;
+    if (ld_flag(abort_a)) return false;
+    if (gtimer() - t0 > tc::WAIT_NS) {
+      asm volatile("st.volatile.shared.u32 [%0], %1;" ::"r"(abort_a), "r"(1) : "memory");
+      atomicExch(&g_ome_timeout, 1);
+      return false;
+    }
+  }
+}
+__device__ __forceinline__ void mbar_arrive32(uint32_t a) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(a) : "memory");
+}
+__device__ __forceinline__ float lds32(uint32_t a) {
+  float v;
+  asm volatile("ld.shared.f32 %0, [%1];" : "=f"(v) : "r"(a));
+  return v;
+}
+__device__ __forceinline__ void sts32(uint32_t a, float v) {
+  asm volatile("st.shared.f32 [%0], %1;" ::"r"(a), "f"(v) : "memory");
+}
+__device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap* map, int x, int y, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::
+          "r"(dst), "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(smem_u32(bar))
+      : "memory");
+}
+__device__ __forceinline__ void tma_load_3d(uint32_t dst, const CUtensorMap* map, int x, int y, int z,
+                                            uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], "
+      "[%5];" ::"r"(dst),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(z), "r"(smem_u32(bar))
+      : "memory");
+}
+__device__ __forceinline__ void umma_bf16_pair(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t acc) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::2.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(d_tmem),
+      "l"(a), "l"(b), "r"(t2::IDESC), "r"(acc));
+}
+// Arrive (once) on the barrier at this shared-memory offset in the CTAs of
+// `mask` when every tcgen05.mma this thread issued so far has completed.
+__device__ __forceinline__ void umma_commit_pair(uint64_t* bar, uint16_t mask) {
+  asm volatile(
+      "tcgen05.commit.cta_group::2.mbarrier::arrive::one.shared::cluster.multicast::cluster.b64 [%0], %1;" ::"r"(
+          smem_u32(bar)),
+      "h"(mask)
+      : "memory");
+}
+__device__ __forceinline__ void tmem_ld8(uint32_t taddr, uint32_t (&r)[8]) {
+  asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+               : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7])
+               : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+__device__ __forceinline__ float4 lds128(uint32_t a) {
+  float4 v;
+  asm volatile("ld.shared.v4.f32 {%0,%1,%2,%3}, [%4];" : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w) : "r"(a));
+  return v;
+}
+__device__ __forceinline__ float2 lds64(uint32_t a) {
+  float2 v;
+  asm volatile("ld.shared.v2.f32 {%0,%1}, [%2];" : "=f"(v.x), "=f"(v.y) : "r"(a));
+  return v;
+}
+// split8 with each term stored (16 bytes at dst + t * TERM_TILE) as soon as
+// it is formed; v is overwritten by the residuals.  The rounding to BF16 is
+// done with integer operations (round half away from zero: add half an ulp of
+// the 8-bit significand, drop the low 16 bits), not with cvt, whose pipe
+// would limit the converter warps; t + (v - t) == v exactly for any rounding
+// of the leading term, so the split stays exact.  Non-finite inputs give
+// NaN residuals.
+template <int NT>
+__device__ __forceinline__ void split8_store(float (&v)[8], uint32_t dst) {
+#pragma unroll
+  for (int t = 0; t < NT; ++t) {
+    uint32_t w[4];
+#pragma unroll
+    for (int p = 0; p < 4; ++p) {
+      const uint32_t ra = __float_as_uint(v[2 * p]) + 0x8000u;
+      const uint32_t rb = __float_as_uint(v[2 * p + 1]) + 0x8000u;
+      w[p] = __byte_perm(ra, rb, 0x7632);   // (ra >> 16) | (rb & 0xffff0000)
+      if (t + 1 < NT) {
+        v[2 * p] -= __uint_as_float(ra & 0xffff0000u);
+        v[2 * p + 1] -= __uint_as_float(rb & 0xffff0000u);
+      }
+    }
+    sts128(dst + t * t2::TERM_TILE, make_uint4(w[0], w[1], w[2], w[3]));
+  }
+}
+
+// Convert one operand's FP32 stage tile (128 rows x 32 k, TMA 128-byte
+// swizzle) into NT BF16 term tiles (K-major canonical: 8-row x 16-byte core
+// matrices, unit (row r, k-chunk c8) at ((r >> 3) * 4 + c8) * 128 + (r & 7) * 16).
+// wl = warp within the operand's 8 warps; each thread converts 2 units.
+// KMAJOR: the tile was loaded as one (32 k, 128 rows) box, row r at r * 128,
+// 16-byte chunk c at (c ^ (r & 7)) * 16.  Otherwise as four (32 rows, 32 k)
+// boxes (rows 32b.., 4 KB each), k-row k at k * 128, chunk c (4 rows) at
+// (c ^ (k & 7)) * 16.
+template <int NT, bool KMAJOR>
+__device__ __forceinline__ void convert_tile(uint32_t f32, uint32_t terms, int wl, int lane) {
+  if constexpr (KMAJOR) {
+#pragma unroll
+    for (int p = 0; p < 2; ++p) {
+      const int r = 8 * (2 * wl + p) + (lane & 7);
+      const int c8 = lane >> 3;
+      const uint32_t base = f32 + (uint32_t)r * 128;
+      const int sw = r & 7;
+      const float4 v0 = lds128(base + ((uint32_t)((2 * c8) ^ sw) << 4));
+      const float4 v1 = lds128(base + ((uint32_t)((2 * c8 + 1) ^ sw) << 4));
+      float v[8] = {v0.x, v0.y, v0.z, v0.w, v1.x, v1.y, v1.z, v1.w};
+      split8_store<NT>(v, terms + (uint32_t)(((r >> 3) * 4 + c8) * 128 + (r & 7) * 16));
+    }
+  } else {
+    const int idx = 2 * wl + (lane >> 4);   // (box, k-chunk) of this half-warp
+    const int b = idx >> 2, c8 = idx & 3;
+    const int rp = lane & 15;               // row pair 2rp, 2rp + 1 of the box
+    float va[8], vb[8];
+#pragma unroll
+    for (int kk = 0; kk < 8; ++kk) {
+      const int k = 8 * c8 + kk;
+      const uint32_t a = f32 + (uint32_t)(b * 4096 + k * 128 + ((((rp >> 1) ^ (k & 7))) << 4) + ((rp & 1) << 3));
+      const float2 v = lds64(a);
+      va[kk] = v.x;
+      vb[kk] = v.y;
+    }
+    // the two rows are stored in an order rotated by lane group so that each
+    // quarter-warp's 16-byte stores hit eight distinct bank groups
+    const int sel = (rp >> 2) & 1;
+    const int r0 = 32 * b + 2 * rp;
+#pragma unroll
+    for (int e = 0; e < 2; ++e) {
+      const int which = e ^ sel;
+      float v[8];
+#pragma unroll
+      for (int kk = 0; kk < 8; ++kk) v[kk] = which ? vb[kk] : va[kk];
+      const int r = r0 + which;
+      split8_store<NT>(v, terms + (uint32_t)(((r >> 3) * 4 + c8) * 128 + (r & 7) * 16));
+    }
+  }
+}
+
+template <int NT, bool AK, bool BKM>
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(t2::NTHREADS, 1)
+    k_gemm_tma2(const __grid_constant__ T2Args t, const __grid_constant__ CUtensorMap mapA,
+                const __grid_constant__ CUtensorMap mapB) {
+  using namespace t2;
+  constexpr int TS = Cfg<NT>::TSTAGES, F32_STAGE = Cfg<NT>::F32_STAGE, TERM_STAGE = Cfg<NT>::TERM_STAGE;
+  extern __shared__ __align__(1024) unsigned char smem_raw[];
+  // 1024-byte aligned base for the 128-byte-swizzled TMA tiles (the same
+  // offset in both CTAs of the pair, which the MMA descriptors rely on)
+  const uint32_t raw = smem_u32(smem_raw);
+  const uint32_t pad = (1024u - (raw & 1023u)) & 1023u;
+  unsigned char* smem = smem_raw + pad;
+  const uint32_t sbase = raw + pad;
+  const uint32_t f32_base = sbase;
+  const uint32_t term_base = sbase + F32_STAGES * F32_STAGE;
+  float* sums_sm = reinterpret_cast<float*>(smem + F32_STAGES * F32_STAGE + TS * TERM_STAGE);
+  uint64_t* bars = reinterpret_cast<uint64_t*>(smem + F32_STAGES * F32_STAGE + TS * TERM_STAGE + Cfg<NT>::SUM_BYTES);
+  uint64_t* f32_full = bars;
+  uint64_t* f32_empty = f32_full + F32_STAGES;
+  uint64_t* term_full = f32_empty + F32_STAGES;   // used in the leader CTA
+  uint64_t* term_empty = term_full + TS;
+  uint64_t* chunk_done = term_empty + TS;
+  uint64_t* drained = chunk_done + 1;             // used in the leader CTA
+  uint64_t* final_bar = drained + 1;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(final_bar + 1);
+  volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
+
+  const GemmArgs& g = t.g;
+  const int tid = threadIdx.x;
+  const int warp = tid >> 5, lane = tid & 31;
+  const uint32_t rank = cluster_rank();
+  const int cid = blockIdx.x >> 1, ncl = gridDim.x >> 1;
+  if (tid == 0) {
+    for (int s = 0; s < F32_STAGES; ++s) {
+      mbar_init(&f32_full[s], 1);
+      mbar_init(&f32_empty[s], 16);
+    }
+    for (int s = 0; s < TS; ++s) {
+      mbar_init(&term_full[s], 32);
+      mbar_init(&term_empty[s], 1);
+    }
+    mbar_init(chunk_done, 1);
+    mbar_init(drained, 32);
+    mbar_init(final_bar, 1);
+    *abort_flag = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 17) {
+    asm volatile("tcgen05.alloc.cta_group::2.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                 "r"(TMEM_COLS)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::2.sync.aligned;" ::: "memory");
+  }
+  tc_fence_before();
+  cluster_sync_all();   // both CTAs' barriers initialised and TMEM allocated
+  tc_fence_after();
+  const uint32_t tmem = *tmem_slot;
+  const uint32_t tmem_main = tmem, tmem_cross = tmem + 256;
+
+  auto decode = [&](int u, int& l, int& mt, int& nt, int& kb, int& ke, int& slot) {
+    int tile;
+    if (u < t.F) {
+      tile = u; kb = 0; ke = t.NKT; slot = -1;
+    } else {
+      const int v = u - t.F;
+      tile = t.F + v / t.S;
+      kb = (v % t.S) * t.ksplit;
+      ke = min(t.NKT, kb + t.ksplit);
+      slot = v;
+    }
+    mt = tile % t.TM;
+    const int r = tile / t.TM;
+    nt = r % t.TN;
+    l = r / t.TN;
+  };
+
+  if (warp == 16) {
+    // ---------------- TMA producer ----------------
+    if (lane == 0) {
+      uint32_t it = 0;
+      bool ok = true;
+      for (int u = cid; u < t.units && ok; u += ncl) {
+        int l, mt, nt, kb, ke, slot;
+        decode(u, l, mt, nt, kb, ke, slot);
+        const int ra = mt * 256 + (int)rank * BM, rb = nt * 256 + (int)rank * BM;
+        for (int kt = kb; kt < ke; ++kt, ++it) {
+          const int s = it % F32_STAGES;
+          if (it >= (uint32_t)F32_STAGES && !mbar_wait(&f32_empty[s], ((it / F32_STAGES) - 1) & 1, abort_flag)) {
+            ok = false;
+            break;
+          }
+          mbar_expect_tx(&f32_full[s], 2 * F32_TILE);
+          const uint32_t da = f32_base + s * F32_STAGE, db = da + F32_TILE;
+          const int k0 = kt * BK;
+          if (g.L > 1) {
+            if (AK) tma_load_3d(da, &mapA, k0, ra, l, &f32_full[s]);
+            else
+              for (int i = 0; i < 4; ++i) tma_load_3d(da + i * 4096, &mapA, ra + 32 * i, k0, l, &f32_full[s]);
+            if (BKM) tma_load_3d(db, &mapB, k0, rb, l, &f32_full[s]);
+            else
+              for (int i = 0; i < 4; ++i) tma_load_3d(db + i * 4096, &mapB, rb + 32 * i, k0, l, &f32_full[s]);
+          } else {
+            if (AK) tma_load_2d(da, &mapA, k0, ra, &f32_full[s]);
+            else
+              for (int i = 0; i < 4; ++i) tma_load_2d(da + i * 4096, &mapA, ra + 32 * i, k0, &f32_full[s]);
+            if (BKM) tma_load_2d(db, &mapB, k0, rb, &f32_full[s]);
+            else
+              for (int i = 0; i < 4; ++i) tma_load_2d(db + i * 4096, &mapB, rb + 32 * i, k0, &f32_full[s]);
+          }
+        }
+      }
+      // this CTA's copies in flight must land before it exits
+      for (uint32_t i = it > (uint32_t)F32_STAGES ? it - F32_STAGES : 0; i < it; ++i)
+        mbar_wait_quiesce(&f32_full[i % F32_STAGES], (i / F32_STAGES) & 1);
+    }
+  } else if (warp == 17) {
+    // ---------------- MMA issue (leader CTA) ----------------
+    if (rank == 0 && lane == 0) {
+      uint32_t it = 0, gc = 0;
+      bool ok = true;
+      for (int u = cid; u < t.units && ok; u += ncl) {
+        int l, mt, nt, kb, ke, slot;
+        decode(u, l, mt, nt, kb, ke, slot);
+        const int nk = ke - kb;
+        for (int j = 0; j < nk; ++j, ++it) {
+          const bool first = j % CHS == 0;
+          if (first && gc >= 1 && !mbar_wait_cl(drained, (gc - 1) & 1, abort_flag)) { ok = false; break; }
+          const int ts = it % TS;
+          if (!mbar_wait_cl(&term_full[ts], (it / TS) & 1, abort_flag)) { ok = false; break; }
+          tc_fence_after();
+          const uint32_t sa = term_base + ts * TERM_STAGE, sb = sa + NT * TERM_TILE;
+#pragma unroll
+          for (int kk = 0; kk < 2; ++kk) {
+            const uint32_t off = kk * 256;
+            uint64_t ad[NT], bd[NT];
+#pragma unroll
+            for (int q = 0; q < NT; ++q) {
+              ad[q] = umma_desc(sa + q * TERM_TILE + off);
+              bd[q] = umma_desc(sb + q * TERM_TILE + off);
+            }
+            const uint32_t keep = (first && kk == 0) ? 0u : 1u;
+            umma_bf16_pair(tmem_main, ad[0], bd[0], keep);
+            bool first_cross = true;
+#pragma unroll
+            for (int d = 1; d < NT; ++d)
+#pragma unroll
+              for (int i = 0; i <= d; ++i) {
+                umma_bf16_pair(tmem_cross, ad[i], bd[d - i], first_cross ? keep : 1u);
+                first_cross = false;
+              }
+          }
+          umma_commit_pair(&term_empty[ts], 3);
+          if (j % CHS == CHS - 1 || j == nk - 1) {
+            umma_commit_pair(chunk_done, 3);
+            ++gc;
+          }
+        }
+      }
+      // every MMA must finish before either CTA frees its TMEM
+      umma_commit_pair(final_bar, 1);
+      mbar_wait_quiesce(final_bar, 0);
+    }
+  } else if (warp < 16) {
+    // ---------------- converters + drain + epilogue (warps 0-15) ----------------
+    const int opnd = warp >> 3, wl = warp & 7;
+    const int q = warp & 3, h = warp >> 2;
+    const int row = 32 * q + lane;                    // accumulator row (TMEM lane) of this thread
+    const int col0 = 64 * h;
+    const uint32_t lane_off = (uint32_t)(32 * q) << 16;
+    // barriers and flags by 32-bit shared address
+    // every address is sbase (or the leader's base) plus a constant, so that
+    // the offsets fold into the instructions instead of taking registers
+    constexpr uint32_t O_BAR = F32_STAGES * F32_STAGE + TS * TERM_STAGE + Cfg<NT>::SUM_BYTES;
+    constexpr uint32_t O_F32_FULL = O_BAR, O_F32_EMPTY = O_BAR + 8 * F32_STAGES;
+    constexpr uint32_t O_TERM_FULL = O_BAR + 8 * 2 * F32_STAGES, O_TERM_EMPTY = O_TERM_FULL + 8 * TS;
+    constexpr uint32_t O_CHUNK_DONE = O_TERM_EMPTY + 8 * TS, O_DRAINED = O_CHUNK_DONE + 8;
+    constexpr uint32_t O_ABORT = O_DRAINED + 8 + 8 + 4;   // after final_bar and the TMEM slot
+    const uint32_t lead = peer_addr(sbase, 0);            // the leader CTA's shared memory, cluster window
+    // running sums of columns col0 .. col0+NSR-1 in registers, the others in
+    // shared memory (thread-contiguous: conflict-free), element j at
+    // ssum + j * NCONV * 4
+    float sum[NSR];
+#pragma unroll
+    for (int j = 0; j < NSR; ++j) sum[j] = 0.f;
+    const uint32_t ssum = sbase + (uint32_t)(F32_STAGES * F32_STAGE + TS * TERM_STAGE) + 4 * tid;
+    // drain cursor: unit du, chunk dci of it, global chunk dgc, its first global stage dstage
+    // (the unit's tile and split are decoded again where needed, which keeps
+    // the cursor at four registers)
+    int du = cid, dci = 0;
+    uint32_t dgc = 0, dstage = 0;
+    auto unit_stages = [&](int u) -> int {
+      if (u < t.F) return t.NKT;
+      const int kb = ((u - t.F) % t.S) * t.ksplit;
+      return min(t.NKT, kb + t.ksplit) - kb;
+    };
+    bool ok = true;
+    auto chunk_end = [&]() -> uint32_t { return dstage + (uint32_t)min((dci + 1) * CHS, unit_stages(du)); };
+    auto drain_one = [&]() -> bool {
+      if (!mbar_wait32(sbase + O_CHUNK_DONE, dgc & 1, sbase + O_ABORT)) return false;
+      tc_fence_after();
+#pragma unroll
+      for (int hh = 0; hh < 8; ++hh) {
+        uint32_t rm[8], rc[8];
+        __syncwarp();
+        tmem_ld8(tmem_main + lane_off + (uint32_t)(col0 + 8 * hh), rm);
+        tmem_ld8(tmem_cross + lane_off + (uint32_t)(col0 + 8 * hh), rc);
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+          const float v = __uint_as_float(rm[j]) + __uint_as_float(rc[j]);
+          const int c = 8 * hh + j;
+          if (c < NSR) {
+            sum[c] = dci == 0 ? v : sum[c] + v;
+          } else {
+            const uint32_t sp = ssum + (uint32_t)((c - NSR) * NCONV * 4);
+            sts32(sp, dci == 0 ? v : lds32(sp) + v);
+          }
+        }
+      }
+      tc_fence_before();
+      __syncwarp();
+      if (lane == 0) mbar_arrive_remote(lead + O_DRAINED);
+      ++dgc;
+      ++dci;
+      const int dn = unit_stages(du);
+      if (dci * CHS >= dn) {
+        // the unit is complete: epilogue
+        int dl, dmt, dnt, dkb, dke, dslot;
+        decode(du, dl, dmt, dnt, dkb, dke, dslot);
+        if (dslot >= 0) {
+          float* pp = t.partial + ((int64_t)dslot * 256 + col0) * 256 + rank * BM + row;
+#pragma unroll
+          for (int j = 0; j < 64; ++j) pp[(int64_t)j * 256] = j < NSR ? sum[j] : lds32(ssum + (uint32_t)((j - NSR) * NCONV * 4));
+        } else {
+          const int64_t m = (int64_t)dmt * 256 + rank * BM + row;
+          if (m < g.M) {
+            const float sx = scalar_as<float>(g.sx), sy = scalar_as<float>(g.sy);
+            float* crow = static_cast<float*>(g.C) + (g.L > 1 ? (int64_t)dl * g.l_sc[0] : 0) + m * g.m_sc[0];
+            const int64_t nsc = g.n_sc[0];
+            const int n0 = dnt * 256 + col0;
+#pragma unroll
+            for (int j = 0; j < 64; ++j) {
+              if (n0 + j < g.N) {
+                float* cp = crow + (int64_t)(n0 + j) * nsc;
+                const float v = j < NSR ? sum[j] : lds32(ssum + (uint32_t)((j - NSR) * NCONV * 4));
+                float o = g.sx_one ? v : sx * v;
+                if (!g.sy_zero) o = fmaf(sy, *cp, o);
+                *cp = o;
+              }
+            }
+          }
+        }
+        dstage += (uint32_t)dn;
+        dci = 0;
+        du += ncl;
+      }
+      return true;
+    };
+
+    uint32_t it = 0;
+    for (int u = cid; u < t.units && ok; u += ncl) {
+      int l, mt, nt, kb, ke, slot;
+      decode(u, l, mt, nt, kb, ke, slot);
+      for (int kt = kb; kt < ke; ++kt, ++it) {
+        // drain every chunk whose MMAs precede the term stage waited on below
+        while (du < t.units && chunk_end() + (uint32_t)TS <= it) {
+          if (!drain_one()) { ok = false; break; }
+        }
+        if (!ok) break;
+        const int s = it % F32_STAGES, ts = it % TS;
+        if (!mbar_wait32(sbase + O_F32_FULL + 8 * s, (it / F32_STAGES) & 1, sbase + O_ABORT)) { ok = false; break; }
+        if (it >= (uint32_t)TS && !mbar_wait32(sbase + O_TERM_EMPTY + 8 * ts, ((it / TS) - 1) & 1, sbase + O_ABORT)) {
+          ok = false;
+          break;
+        }
+        const uint32_t src = f32_base + s * F32_STAGE + opnd * F32_TILE;
+        const uint32_t dst = term_base + ts * TERM_STAGE + opnd * NT * TERM_TILE;
+        if (opnd == 0) convert_tile<NT, AK>(src, dst, wl, lane);
+        else convert_tile<NT, BKM>(src, dst, wl, lane);
+        fence_proxy_async();
+        __syncwarp();
+        if (lane == 0) {
+          mbar_arrive32(sbase + O_F32_EMPTY + 8 * s);
+          mbar_arrive_remote(lead + O_TERM_FULL + 8 * ts);
+        }
+      }
+    }
+    while (ok && du < t.units) ok = drain_one();
+  }
+  tc_fence_before();
+  __syncthreads();
+  cluster_sync_all();   // the peer's drains and the leader's MMAs are over
+  if (warp == 17) {
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::2.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(t2::TMEM_COLS) : "memory");
+  }
+}
+
+// Sum the S split partials of each split 256 x 256 tile in split order; αβ epilogue.
+__global__ void __launch_bounds__(256) k_splitk_tiles2(const __grid_constant__ T2Args t) {
+  const GemmArgs& g = t.g;
+  const float sx = scalar_as<float>(g.sx), sy = scalar_as<float>(g.sy);
+  float* Cp = static_cast<float*>(g.C);
+  const int64_t total = (int64_t)(t.tiles - t.F) * 256 * 256;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t mloc = i % 256;
+    const int64_t r = i / 256;
+    const int64_t nloc = r % 256;
+    const int64_t v = r / 256;
+    const int64_t tile = t.F + v;
+    const int64_t mt = tile % t.TM, r2 = tile / t.TM, nt = r2 % t.TN, l = r2 / t.TN;
+    const int64_t m = mt * 256 + mloc, n = nt * 256 + nloc;
+    if (m >= g.M || n >= g.N) continue;
+    float acc = 0.f;
+    for (int s = 0; s < t.S; ++s) acc += t.partial[((v * t.S + s) * 256 + nloc) * 256 + mloc];
+    float* cp = Cp + (g.L > 1 ? l * g.l_sc[0] : 0) + m * g.m_sc[0] + n * g.n_sc[0];
+    float o = g.sx_one ? acc : sx * acc;
+    if (!g.sy_zero) o = fmaf(sy, *cp, o);
+    *cp = o;
+  }
+}
+
+namespace {
+typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                  const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+EncodeTiledFn encode_fn() {
+  static EncodeTiledFn fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<EncodeTiledFn>(p);
+    else
+      cudaGetLastError();
+  });
+  return fn;
+}
+
+// Tensor map over one FP32 operand: rows R (stride rs), K (stride ks), batch
+// L (stride ls; L == 1: a 2-D map).  kmajor (ks == 1): box (32 k, 128 rows);
+// otherwise (rs == 1): box (32 rows, 32 k).  128-byte swizzle, zero fill.
+bool make_operand_map(CUtensorMap* map, const void* base, int64_t R, int64_t K, int64_t L, int64_t rs, int64_t ks,
+                      int64_t ls, bool kmajor) {
+  EncodeTiledFn fn = encode_fn();
+  if (!fn) return false;
+  cuuint64_t dims[3], strides[2];
+  cuuint32_t box[3], estr[3] = {1, 1, 1};
+  if (kmajor) {
+    dims[0] = (cuuint64_t)K; dims[1] = (cuuint64_t)R;
+    strides[0] = (cuuint64_t)rs * 4;
+    box[0] = 32; box[1] = 128;
+  } else {
+    dims[0] = (cuuint64_t)R; dims[1] = (cuuint64_t)K;
+    strides[0] = (cuuint64_t)ks * 4;
+    box[0] = 32; box[1] = 32;
+  }
+  dims[2] = (cuuint64_t)L;
+  strides[1] = (cuuint64_t)ls * 4;
+  box[2] = 1;
+  const cuuint32_t rank = L > 1 ? 3 : 2;
+  CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, rank, const_cast<void*>(base), dims, strides, box, estr,
+                  CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                  CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS;
+}
+
+template <int NT, bool AK, bool BKM>
+cudaError_t launch_t2(const T2Args& t, const CUtensorMap& ma, const CUtensorMap& mb, int grid, cudaStream_t s) {
+  static bool attr = false;
+  if (!attr) {
+    cudaError_t e = cudaFuncSetAttribute(k_gemm_tma2<NT, AK, BKM>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         t2::Cfg<NT>::SMEM_BYTES);
+    if (e != cudaSuccess) return e;
+    attr = true;
+  }
+  k_gemm_tma2<NT, AK, BKM><<<grid, t2::NTHREADS, t2::Cfg<NT>::SMEM_BYTES, s>>>(t, ma, mb);
+  return cudaGetLastError();
+}
+}  // namespace
+
+bool gemm_tma2_applies(const GemmArgs& g) {
+  if (g.nm != 1 || g.nn != 1 || g.nk != 1 || g.nl != 1) return false;
+  if (g.M < 1 || g.N < 1 || g.K < 1 || g.L < 1) return false;
+  if (g.M >= (1ll << 31) || g.N >= (1ll << 31) || g.K >= (1ll << 31) || g.L >= (1ll << 31)) return false;
+  const bool ak = g.k_sa[0] == 1, ar = g.m_sa[0] == 1;
+  const bool bk = g.k_sb[0] == 1, br = g.n_sb[0] == 1;
+  if (!(ak || ar) || !(bk || br)) return false;
+  // tensor-map rules: 16-byte aligned bases and non-unit strides of whole 16-byte units
+  if ((reinterpret_cast<uintptr_t>(g.A) & 15) || (reinterpret_cast<uintptr_t>(g.B) & 15)) return false;
+  const int64_t sa = ak ? g.m_sa[0] : g.k_sa[0], sb = bk ? g.n_sb[0] : g.k_sb[0];
+  if (sa <= 0 || sb <= 0 || sa % 4 || sb % 4 || sa >= (1ll << 37) || sb >= (1ll << 37)) return false;
+  if (g.L > 1 && (g.l_sa[0] <= 0 || g.l_sb[0] <= 0 || g.l_sa[0] % 4 || g.l_sb[0] % 4 ||
+                  g.l_sa[0] >= (1ll << 37) || g.l_sb[0] >= (1ll << 37)))
+    return false;
+  return true;
+}
+
+size_t gemm_tma2_bytes(const GemmArgs& g, int num_sms) {
+  (void)g;
+  return (size_t)(num_sms / 2) * 256 * 256 * 4 + 1024;
+}
+
+cudaError_t launch_gemm_tma2(const GemmArgs& g, int nterms, void* workspace, size_t ws_bytes, int num_sms,
+                             cudaStream_t s) {
+  if ((nterms != 2 && nterms != 3) || !gemm_tma2_applies(g)) return cudaErrorNotSupported;
+  const bool ak = g.k_sa[0] == 1, bk = g.k_sb[0] == 1;
+  alignas(64) CUtensorMap ma, mb;
+  if (!make_operand_map(&ma, g.A, g.M, g.K, g.L, g.m_sa[0], g.k_sa[0], g.L > 1 ? g.l_sa[0] : 0, ak) ||
+      !make_operand_map(&mb, g.B, g.N, g.K, g.L, g.n_sb[0], g.k_sb[0], g.L > 1 ? g.l_sb[0] : 0, bk))
+    return cudaErrorNotSupported;
+  const int64_t TM = (g.M + 255) / 256, TN = (g.N + 255) / 256, NKT = (g.K + t2::BK - 1) / t2::BK;
+  const int64_t tiles = g.L * TM * TN;
+  const int64_t G = std::max(1, num_sms / 2);   // clusters of two CTAs
+  int64_t F = tiles >= G ? (tiles / G) * G : 0;
+  int64_t Rt = tiles - F;
+  int64_t S = 1;
+  if (Rt > 0) {
+    S = std::max<int64_t>(1, G / Rt);
+    S = std::min<int64_t>(S, std::max<int64_t>(1, NKT / 8));
+  }
+  const int64_t ksplit = (NKT + S - 1) / S;
+  S = (NKT + ksplit - 1) / ksplit;
+  if (S == 1) {
+    F = tiles;
+    Rt = 0;
+  }
+  const int64_t units = F + Rt * S;
+  // the kernel's unit, tile and stage counters are 32-bit
+  if (tiles >= (1ll << 30) || units >= (1ll << 30) || NKT >= (1ll << 30)) return cudaErrorNotSupported;
+  const size_t bytes_p = (size_t)Rt * S * 256 * 256 * 4;
+  if (bytes_p > ws_bytes) return cudaErrorNotSupported;
+  T2Args t;
+  memset(&t, 0, sizeof(t));
+  t.g = g;
+  t.TM = (int)TM;
+  t.TN = (int)TN;
+  t.NKT = (int)NKT;
+  t.tiles = (int)tiles;
+  t.partial = static_cast<float*>(workspace);
+  t.F = (int)F;
+  t.S = (int)S;
+  t.ksplit = (int)ksplit;
+  t.units = (int)units;
+  const int grid = (int)(2 * std::min<int64_t>(units, G));
+  cudaError_t e;
+  {
+    KernelTimer kt(s, "k_gemm_tma2");
+    if (nterms == 3) {
+      e = ak ? (bk ? launch_t2<3, true, true>(t, ma, mb, grid, s) : launch_t2<3, true, false>(t, ma, mb, grid, s))
+             : (bk ? launch_t2<3, false, true>(t, ma, mb, grid, s) : launch_t2<3, false, false>(t, ma, mb, grid, s));
+    } else {
+      e = ak ? (bk ? launch_t2<2, true, true>(t, ma, mb, grid, s) : launch_t2<2, true, false>(t, ma, mb, grid, s))
+             : (bk ? launch_t2<2, false, true>(t, ma, mb, grid, s) : launch_t2<2, false, false>(t, ma, mb, grid, s));
+    }
+  }
+  count_launch();
+  if (e != cudaSuccess || Rt == 0) return e;
+  const int64_t total = Rt * 256 * 256;
+  const int64_t nb = (total + 255) / 256;
+  k_splitk_tiles2<<<(unsigned)std::min<int64_t>(nb, (int64_t)num_sms * 16), 256, 0, s>>>(t);
   count_launch();
   return cudaGetLastError();
 }

@@ -94,6 +94,14 @@ cudaError_t launch_c_offsets(GemmArgs& g, int64_t* tab, cudaStream_t s);
 cudaError_t launch_gemm_packed(const GemmArgs& g, int nterms, void* workspace, size_t ws_bytes, int num_sms,
                                cudaStream_t s, int64_t* ctab);
 size_t gemm_packed_bytes(const GemmArgs& g, int nterms, int num_sms);
+// 2-SM tensor-core GEMM fed by TMA tensor maps over the FP32 operands (BF16
+// terms formed in shared memory): single-mode M, N, K and batch groups, each
+// operand contiguous along its row or K mode, 16-byte aligned.  Split-K
+// partials go to `workspace`; cudaErrorNotSupported (nothing launched) when
+// the shape or the workspace does not fit.
+bool gemm_tma2_applies(const GemmArgs& g);
+cudaError_t launch_gemm_tma2(const GemmArgs& g, int nterms, void* workspace, size_t ws_bytes, int num_sms,
+                             cudaStream_t s);
 
 // Synchronise s and read/clear the device timeout flag: 1 if a bounded wait
 // gave up, 0 if not, -cudaError on failure.

@@ -32,8 +32,8 @@ pytestmark = pytest.mark.gpu
 
 # main kernel per suite case: FP32, Int64
 MAIN_KERNEL = {
-    "abcd,cdef->abef": ("k_gemm_packed", "k_gemm_simt"),
-    "ijk,jkl->il": ("k_gemm_packed", "k_gemm_simt"),
+    "abcd,cdef->abef": ("k_gemm_tma2", "k_gemm_simt"),
+    "ijk,jkl->il": ("k_gemm_tma2", "k_gemm_simt"),
     "bij,bjk->bik": ("k_gemm_bstage", "k_gemm_bstage"),
     "abcde->ecadb": ("k_transpose_v4", "k_transpose32"),
     "ii->": ("k_loop_block", "k_loop_block"),

@@ -203,15 +203,70 @@ def test_large_gemm_packed(code, sizes):
     assert_match(got, oracle(ixs, iy, xs, sizes, "f32", wide=True), "f32", 1e-6)
 
 
+def kernel_names(fn):
+    """Run fn() with the library's kernel-event record on; (result, main kernel names)."""
+    import ctypes as C
+    from omeinsum_b200 import _lib
+    lib = _lib.load()
+    lib.ome_kernel_timing(16)
+    try:
+        out = fn()
+        torch.cuda.synchronize()
+        ome.device_status()
+        ms = (C.c_float * 16)()
+        names = (C.c_char_p * 16)()
+        cnt = C.c_int32()
+        lib.ome_kernel_times(16, ms, names, C.byref(cnt))
+    finally:
+        lib.ome_kernel_timing(0)
+    return out, [names[i].decode() for i in range(cnt.value)]
+
+
+@pytest.mark.parametrize("prec,rtol", [(3, 1e-6), (2, 1e-5)])
+@pytest.mark.parametrize("code,sizes", [
+    ("ij,jk->ik", dict(i=300, j=520, k=700)),          # A row-major (M contiguous), B K-major; ragged M, N, K
+    ("ji,jk->ik", dict(i=260, j=1000, k=390)),         # both K-major
+    ("ij,kj->ik", dict(i=512, j=776, k=640)),          # A row-major, B row-major (N contiguous)
+    ("ji,kj->ik", dict(i=384, j=1000, k=300)),         # A K-major, B row-major
+    ("ijl,jkl->ikl", dict(i=256, j=1024, k=256, l=3)),  # batched: 3-D tensor maps
+    ("ij,jk->ik", dict(i=2560, j=320, k=2560)),        # a whole wave of cluster tiles + a split remainder
+    ("ij,jk->ik", dict(i=256, j=16384, k=256)),        # one tile split along K over every cluster
+])
+def test_gemm_tma2(code, sizes, prec, rtol):
+    """The 2-SM tensor-core GEMM fed by tensor maps over the FP32 operands
+    (BF16 terms formed in shared memory) against FP64, in every operand
+    orientation, with y <- 2y + 3f on a second call."""
+    rng = np.random.default_rng(31)
+    ixs, iy = parse(code)
+    xs = [gen(rng, [sizes[l] for l in ix], "f32") for ix in ixs]
+    c = ome.EinCode(ixs, iy)
+    dxs = [to_dev(x, "f32") for x in xs]
+    want = oracle(ixs, iy, xs, sizes, "f32", wide=True)
+    ome.set_einsum_backend(ome.B200Backend(prec=prec))
+    try:
+        got, names = kernel_names(lambda: ome.einsum(c, dxs, sizes))
+        assert names == ["k_gemm_tma2"], names
+        assert_match(to_np(got), want, "f32", rtol)
+        y0 = gen(rng, [sizes[l] for l in iy], "f32")
+        yd = to_dev(y0, "f32")
+        ome.einsum_(c, dxs, yd, 3, 2, sizes)
+        ome.device_status()
+        assert_match(to_np(yd), 3 * want + 2 * y0.astype(np.float64), "f32", rtol)
+    finally:
+        ome.set_einsum_backend(ome.B200Backend())
+
+
 def test_packed_gemm_overflow_scratch():
-    """A GEMM whose BF16 operand terms (805 MB for M = N = 1024, K = 65536)
-    exceed the 256 MiB default workspace still runs on the packed kernel,
-    through the context's overflow scratch, and matches FP64."""
+    """A GEMM whose BF16 operand terms (804 MB for M = 1023, N = 1024,
+    K = 65536) exceed the 256 MiB default workspace still runs on the packed
+    kernel (a K stride of 1023 elements is not a whole number of 16-byte
+    units, which the tensor-map kernel needs), through the context's overflow
+    scratch, and matches FP64."""
     import ctypes as C
     from omeinsum_b200 import _lib
     _lib.release_workspaces()
     torch.manual_seed(3)
-    a = torch.randn(1024, 65536, dtype=torch.float32, device="cuda")
+    a = torch.randn(1023, 65536, dtype=torch.float32, device="cuda")
     b = torch.randn(65536, 1024, dtype=torch.float32, device="cuda")
     A, B = a.t().contiguous().t(), b.t().contiguous().t()   # column-major
     lib = _lib.load()
