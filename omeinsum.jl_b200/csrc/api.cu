@@ -721,7 +721,11 @@ static int run_binary(ome_ctx* ctx, cudaStream_t s, ome_dtype dt, HView x1, HVie
       cudaGetLastError();
     }
     trace_path("  -> simt");
-    return cuda_err(launch_gemm_simt(dt, g, s), "simt gemm");
+    // split-K partials (long K, few tiles) go to the free workspace above ws_top
+    const size_t off = (ctx->ws_top + 255) & ~(size_t)255;
+    const size_t free_bytes = ctx->ws_bytes > off ? ctx->ws_bytes - off : 0;
+    return cuda_err(launch_gemm_simt_ws(dt, g, free_bytes ? ctx->ws + off : nullptr, free_bytes, ctx->num_sms, s),
+                    "simt gemm");
   }
   HView xs[2] = {x1, x2};
   if (trace_on()) {

@@ -27,8 +27,19 @@ __device__ __forceinline__ int64_t group_off(int64_t i, int n, const int64_t* ex
   return mode_offset(i, n, ext, str);
 }
 
+// Split along K (for grids too small to fill the GPU): blockIdx.z runs over
+// L x S, block (l, sp) sums k in [sp * kchunk, (sp + 1) * kchunk) and writes
+// its tile to partial[((sp * L + l) * M + m) * N + n]; k_simt_splitk_finish
+// adds the S partials in split order and applies the epilogue.
+struct SimtSplit {
+  int S;               // 1: no split
+  int64_t kchunk;
+  void* partial;
+};
+
 template <class A, class C = SimtCfg<sizeof(typename A::T)>>
-__global__ void __launch_bounds__(256) k_gemm_simt(const __grid_constant__ GemmArgs g) {
+__global__ void __launch_bounds__(256) k_gemm_simt(const __grid_constant__ GemmArgs g,
+                                                    const __grid_constant__ SimtSplit sp) {
   using T = typename A::T;
   constexpr int BM = C::BM, BN = C::BN, BK = C::BK, TM = C::TM, TN = C::TN;
   constexpr int NT = 256;
@@ -46,7 +57,11 @@ __global__ void __launch_bounds__(256) k_gemm_simt(const __grid_constant__ GemmA
   const int tx = tid % (BN / TN), ty = tid / (BN / TN);
   const int64_t m0 = (int64_t)blockIdx.x * BM, n0 = (int64_t)blockIdx.y * BN;
 
-  for (int64_t l = blockIdx.z; l < g.L; l += gridDim.z) {
+  const int64_t zsteps = g.L * sp.S;
+  for (int64_t z = blockIdx.z; z < zsteps; z += gridDim.z) {
+    const int64_t l = z % g.L, spi = z / g.L;
+    const int64_t kbeg = spi * sp.kchunk;
+    const int64_t kend = sp.S > 1 ? min(g.K, kbeg + sp.kchunk) : g.K;
     const int64_t la = mode_offset(l, g.nl, g.l_ext, g.l_sa);
     const int64_t lb = mode_offset(l, g.nl, g.l_ext, g.l_sb);
     const int64_t lc = mode_offset(l, g.nl, g.l_ext, g.l_sc);
@@ -71,7 +86,7 @@ __global__ void __launch_bounds__(256) k_gemm_simt(const __grid_constant__ GemmA
         const int kk = g.a_m_fast ? e / BM : e % BK;
         const int64_t k = k0 + kk;
         const int64_t base = am[mm];
-        ra[r] = (base >= 0 && k < g.K) ? Ap[base + group_off(k, g.nk, g.k_ext, g.k_sa)] : A::zero();
+        ra[r] = (base >= 0 && k < kend) ? Ap[base + group_off(k, g.nk, g.k_ext, g.k_sa)] : A::zero();
       }
 #pragma unroll
       for (int r = 0; r < RB; ++r) {
@@ -80,7 +95,7 @@ __global__ void __launch_bounds__(256) k_gemm_simt(const __grid_constant__ GemmA
         const int kk = g.b_n_fast ? e / BN : e % BK;
         const int64_t k = k0 + kk;
         const int64_t base = bn[nn];
-        rb[r] = (base >= 0 && k < g.K) ? Bp[base + group_off(k, g.nk, g.k_ext, g.k_sb)] : A::zero();
+        rb[r] = (base >= 0 && k < kend) ? Bp[base + group_off(k, g.nk, g.k_ext, g.k_sb)] : A::zero();
       }
     };
     auto store = [&](int buf) {
@@ -100,12 +115,12 @@ __global__ void __launch_bounds__(256) k_gemm_simt(const __grid_constant__ GemmA
       }
     };
 
-    load(0);
+    load(kbeg);
     store(0);
     __syncthreads();
     int buf = 0;
-    for (int64_t k0 = 0; k0 < g.K; k0 += BK) {
-      const bool more = k0 + BK < g.K;
+    for (int64_t k0 = kbeg; k0 < kend; k0 += BK) {
+      const bool more = k0 + BK < kend;
       if (more) load(k0 + BK);
 #pragma unroll
       for (int kk = 0; kk < BK; ++kk) {
@@ -135,15 +150,45 @@ __global__ void __launch_bounds__(256) k_gemm_simt(const __grid_constant__ GemmA
       const int64_t n = n0 + tx * TN + j;
       cn[j] = n < g.N ? group_off(n, g.nn, g.n_ext, g.n_sc) : -1;
     }
+    if (sp.S > 1) {
+      T* pp = static_cast<T*>(sp.partial) + (spi * g.L + l) * g.M * g.N;
 #pragma unroll
-    for (int i = 0; i < TM; ++i)
+      for (int i = 0; i < TM; ++i)
 #pragma unroll
-      for (int j = 0; j < TN; ++j)
-        if (cm[i] >= 0 && cn[j] >= 0) {
-          T* cp = Cp + lc + cm[i] + cn[j];
-          *cp = epilogue<A>(acc[i][j], cp, sx, sy, g.sy_zero, g.sx_one);
+        for (int j = 0; j < TN; ++j) {
+          const int64_t m = m0 + ty * TM + i, n = n0 + tx * TN + j;
+          if (m < g.M && n < g.N) pp[m * g.N + n] = acc[i][j];
         }
+    } else {
+#pragma unroll
+      for (int i = 0; i < TM; ++i)
+#pragma unroll
+        for (int j = 0; j < TN; ++j)
+          if (cm[i] >= 0 && cn[j] >= 0) {
+            T* cp = Cp + lc + cm[i] + cn[j];
+            *cp = epilogue<A>(acc[i][j], cp, sx, sy, g.sy_zero, g.sx_one);
+          }
+    }
     __syncthreads();
+  }
+}
+
+// Sum the S split partials of every output in split order; αβ epilogue.
+template <class A>
+__global__ void __launch_bounds__(256) k_simt_splitk_finish(const __grid_constant__ GemmArgs g,
+                                                             const __grid_constant__ SimtSplit sp) {
+  using T = typename A::T;
+  const T* pp = static_cast<const T*>(sp.partial);
+  T* Cp = static_cast<T*>(g.C);
+  const T sx = scalar_as<T>(g.sx), sy = scalar_as<T>(g.sy);
+  const int64_t per = g.L * g.M * g.N;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < per; i += (int64_t)gridDim.x * blockDim.x) {
+    T acc = pp[i];
+    for (int s = 1; s < sp.S; ++s) acc = A::add(acc, pp[s * per + i]);
+    const int64_t n = i % g.N, r = i / g.N, m = r % g.M, l = r / g.M;
+    T* cp = Cp + mode_offset(l, g.nl, g.l_ext, g.l_sc) + group_off(m, g.nm, g.m_ext, g.m_sc) +
+            group_off(n, g.nn, g.n_ext, g.n_sc);
+    *cp = epilogue<A>(acc, cp, sx, sy, g.sy_zero, g.sx_one);
   }
 }
 
@@ -152,10 +197,45 @@ static cudaError_t launch_gemm_simt_t(const GemmArgs& g, cudaStream_t s) {
   using C = SimtCfg<sizeof(typename A::T)>;
   const int64_t gm = (g.M + C::BM - 1) / C::BM, gn = (g.N + C::BN - 1) / C::BN;
   if (gm > 0x7fffffff || gn > 65535) return cudaErrorNotSupported;
+  SimtSplit sp{1, g.K, nullptr};
   const int64_t gl = g.L < 65535 ? g.L : 65535;
   dim3 grid((unsigned)gm, (unsigned)gn, (unsigned)gl);
   KernelTimer kt(s, "k_gemm_simt");
-  k_gemm_simt<A><<<grid, 256, 0, s>>>(g); count_launch();
+  k_gemm_simt<A><<<grid, 256, 0, s>>>(g, sp); count_launch();
+  return cudaGetLastError();
+}
+
+// The same with K split over blocks when the tiles alone would leave most
+// SMs idle (long K, few tiles) and the partials fit `workspace`.
+template <class A>
+static cudaError_t launch_gemm_simt_ws_t(const GemmArgs& g, void* workspace, size_t ws_bytes, int num_sms,
+                                         cudaStream_t s) {
+  using T = typename A::T;
+  using C = SimtCfg<sizeof(T)>;
+  const int64_t gm = (g.M + C::BM - 1) / C::BM, gn = (g.N + C::BN - 1) / C::BN;
+  const int64_t blocks = gm * gn * g.L;
+  int64_t S = 1;
+  if (blocks < num_sms && g.K >= 1024 && gn <= 65535 && gm <= 0x7fffffff) {
+    S = std::min<int64_t>((2 * (int64_t)num_sms + blocks - 1) / blocks, g.K / 256);
+    S = std::min<int64_t>(S, 65535 / std::max<int64_t>(g.L, 1));
+    while (S > 1 && (size_t)S * g.L * g.M * g.N * sizeof(T) > ws_bytes) --S;
+  }
+  if (S <= 1) return launch_gemm_simt_t<A>(g, s);
+  const int64_t kchunk = (g.K + S - 1) / S;
+  S = (g.K + kchunk - 1) / kchunk;
+  SimtSplit sp{(int)S, kchunk, workspace};
+  dim3 grid((unsigned)gm, (unsigned)gn, (unsigned)(g.L * S));
+  {
+    KernelTimer kt(s, "k_gemm_simt");
+    k_gemm_simt<A><<<grid, 256, 0, s>>>(g, sp);
+  }
+  count_launch();
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  const int64_t per = g.L * g.M * g.N;
+  const int64_t nb = std::min<int64_t>((per + 255) / 256, (int64_t)num_sms * 16);
+  k_simt_splitk_finish<A><<<(unsigned)nb, 256, 0, s>>>(g, sp);
+  count_launch();
   return cudaGetLastError();
 }
 
@@ -374,9 +454,16 @@ cudaError_t launch_gemm_simt_small_f32(const GemmArgs& g, cudaStream_t s) {
   if (g.M > SimtSmall::BM || g.N > SimtSmall::BN) return cudaErrorNotSupported;
   const int64_t gl = g.L < 65535 ? g.L : 65535;
   KernelTimer kt(s, "k_gemm_simt");
-  k_gemm_simt<AlgF32, SimtSmall><<<dim3(1, 1, (unsigned)gl), 256, 0, s>>>(g);
+  k_gemm_simt<AlgF32, SimtSmall><<<dim3(1, 1, (unsigned)gl), 256, 0, s>>>(g, SimtSplit{1, g.K, nullptr});
   count_launch();
   return cudaGetLastError();
+}
+
+cudaError_t launch_gemm_simt_ws(ome_dtype dt, const GemmArgs& g, void* workspace, size_t ws_bytes, int num_sms,
+                                cudaStream_t s) {
+  cudaError_t e = cudaErrorInvalidValue;
+  OME_DISPATCH(dt, ALG, e = launch_gemm_simt_ws_t<ALG>(g, workspace, ws_bytes, num_sms, s));
+  return e;
 }
 
 cudaError_t launch_gemm_simt(ome_dtype dt, const GemmArgs& g, cudaStream_t s) {

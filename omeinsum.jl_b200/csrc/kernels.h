@@ -53,6 +53,10 @@ cudaError_t launch_scale(ome_dtype dt, void* y, int nd, const int64_t* ext, cons
 
 // CUDA-core strided batched GEMM over any algebra.
 cudaError_t launch_gemm_simt(ome_dtype dt, const GemmArgs& g, cudaStream_t s);
+// The same, with K split over blocks (partials in `workspace`, summed in
+// split order) when the output tiles alone would leave most SMs idle.
+cudaError_t launch_gemm_simt_ws(ome_dtype dt, const GemmArgs& g, void* workspace, size_t ws_bytes, int num_sms,
+                                cudaStream_t s);
 // FP32 batched GEMM with M, N <= 64 on CUDA cores (64 x 64 tiles, one per batch).
 cudaError_t launch_gemm_simt_small_f32(const GemmArgs& g, cudaStream_t s);
 // Batched GEMM with the batch mode contiguous in A, B and C and M, N <= 64

@@ -434,3 +434,32 @@ def test_mixed_eltype_inputs(code, dts, want_dtype):
     tgt = {torch.float32: "f32", torch.float64: "f64", torch.int64: "i64", torch.complex64: "c64",
            torch.complex128: "c128"}[want_dtype]
     assert_match(to_np(got), want, tgt)
+
+
+@pytest.mark.parametrize("dt", ["f64", "c64", "i64", "trop", "bool", "f32"])
+@pytest.mark.parametrize("code,sizes", [
+    ("ij,jk->ik", dict(i=100, j=20000, k=90)),          # a 2 x 2 grid of tiles: K split over blocks
+    ("ijl,jkl->ikl", dict(i=70, j=5000, k=60, l=2)),    # batched
+    ("ji,kj->ik", dict(i=130, j=3000, k=33)),           # transposed operands, ragged tiles
+])
+def test_cuda_core_gemm_split_k(code, sizes, dt):
+    """CUDA-core GEMMs with a long K and few output tiles split K over blocks
+    (partials summed in split order): FP64, complex, Int64, max-plus, Bool and
+    plain FP32, with y <- 3y + 2f."""
+    rng = np.random.default_rng(41)
+    ixs, iy = parse(code)
+    xs = [gen(rng, [sizes[l] for l in ix], dt) for ix in ixs]
+    c = ome.EinCode(ixs, iy)
+    if dt == "f32":
+        ome.set_einsum_backend(ome.B200Backend(prec=1))
+    try:
+        got, names = kernel_names(lambda: ome.einsum(c, [to_dev(x, dt) for x in xs], sizes))
+        assert names == ["k_gemm_simt"], names
+        assert_match(to_np(got), oracle(ixs, iy, xs, sizes, dt), dt)
+        if dt == "i64":
+            y0 = gen(rng, [sizes[l] for l in iy], dt)
+            yd = to_dev(y0, dt)
+            ome.einsum_(c, [to_dev(x, dt) for x in xs], yd, 2, 3, sizes)
+            assert_match(to_np(yd), 2 * oracle(ixs, iy, xs, sizes, dt) + 3 * y0, dt)
+    finally:
+        ome.set_einsum_backend(ome.B200Backend())
