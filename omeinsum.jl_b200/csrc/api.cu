@@ -672,6 +672,14 @@ static int run_binary(ome_ctx* ctx, cudaStream_t s, ome_dtype dt, HView x1, HVie
                (long long)N, (long long)K, (long long)L, gm.n, gn.n, gk.n, gl.n, g.a_m_fast, g.b_n_fast, prec);
     // batches of small GEMMs with the batch mode innermost in every tensor
     // (column-major bij,bjk->bik): lanes over consecutive batches
+    if (dt == OME_F32 && prec != OME_PREC_FP32 && gemm_bdiag_applies(g)) {
+      cudaError_t e = launch_gemm_bdiag(g, prec == OME_PREC_BF16X3 ? 2 : 3, s);
+      if (e != cudaErrorNotSupported) {
+        trace_path("  -> batch-innermost tensor cores");
+        return cuda_err(e, "batch-innermost tensor-core gemm");
+      }
+      cudaGetLastError();
+    }
     if (gemm_bfast_applies(g)) {
       trace_path("  -> batch-innermost");
       return cuda_err(launch_gemm_bfast(dt, g, s), "batch-innermost gemm");
@@ -796,14 +804,14 @@ int einsum_views(ome_ctx* ctx, cudaStream_t s, ome_dtype dt, int nin, const HVie
   cudaEventRecord(e0, s);
   const int rc = einsum_views_impl(ctx, s, dt, nin, xs, y, sx, sy, prec, loop_only);
   cudaEventRecord(e1, s);
-  cudaEventSynchronize(e1);
+  const cudaError_t se = cudaEventSynchronize(e1);
   float ms = 0.f;
   cudaEventElapsedTime(&ms, e0, e1);
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   fprintf(stderr, "[ome] dt=%d nin=%d ranks=", (int)dt, nin);
   for (int i = 0; i < nin; ++i) fprintf(stderr, "%d,", xs[i].nd);
-  fprintf(stderr, "%d us=%.1f %s\n", y.nd, ms * 1e3, g_trace);
+  fprintf(stderr, "%d us=%.1f err=%d %s\n", y.nd, ms * 1e3, (int)se, g_trace);
   return rc;
 }
 
@@ -824,6 +832,8 @@ unsigned long long ome_launch_count(void) { return ome::launch_counter(); }
 int ome_device_status(void* stream) {
   const int r = ome::device_status(static_cast<cudaStream_t>(stream));
   if (r < 0) return cuda_err((cudaError_t)(-r), "device status");
+  if (r > 100)
+    return set_err(OME_CUDA_ERROR, "kernel self-check %d: an output offset outside the view was skipped", r - 100);
   if (r > 0) return set_err(OME_TIMEOUT, "a device-side wait gave up (bounded wait expired)");
   return OME_OK;
 }

@@ -35,7 +35,10 @@ struct SimtSplit {
   int S;               // 1: no split
   int64_t kchunk;
   void* partial;
+  int64_t p_elems;     // partial capacity in elements (self-check)
 };
+// set (5) when a split partial's offset falls outside the scratch (self-check)
+__device__ int g_ome_bounds_simt = 0;
 
 template <class A, class C = SimtCfg<sizeof(typename A::T)>>
 __global__ void __launch_bounds__(256) k_gemm_simt(const __grid_constant__ GemmArgs g,
@@ -157,7 +160,11 @@ __global__ void __launch_bounds__(256) k_gemm_simt(const __grid_constant__ GemmA
 #pragma unroll
         for (int j = 0; j < TN; ++j) {
           const int64_t m = m0 + ty * TM + i, n = n0 + tx * TN + j;
-          if (m < g.M && n < g.N) pp[m * g.N + n] = acc[i][j];
+          if (m < g.M && n < g.N) {
+            const int64_t po = (spi * g.L + l) * g.M * g.N + m * g.N + n;
+            if (po < sp.p_elems) pp[m * g.N + n] = acc[i][j];
+            else atomicCAS(&g_ome_bounds_simt, 0, 5);
+          }
         }
     } else {
 #pragma unroll
@@ -197,7 +204,7 @@ static cudaError_t launch_gemm_simt_t(const GemmArgs& g, cudaStream_t s) {
   using C = SimtCfg<sizeof(typename A::T)>;
   const int64_t gm = (g.M + C::BM - 1) / C::BM, gn = (g.N + C::BN - 1) / C::BN;
   if (gm > 0x7fffffff || gn > 65535) return cudaErrorNotSupported;
-  SimtSplit sp{1, g.K, nullptr};
+  SimtSplit sp{1, g.K, nullptr, 0};
   const int64_t gl = g.L < 65535 ? g.L : 65535;
   dim3 grid((unsigned)gm, (unsigned)gn, (unsigned)gl);
   KernelTimer kt(s, "k_gemm_simt");
@@ -223,7 +230,7 @@ static cudaError_t launch_gemm_simt_ws_t(const GemmArgs& g, void* workspace, siz
   if (S <= 1) return launch_gemm_simt_t<A>(g, s);
   const int64_t kchunk = (g.K + S - 1) / S;
   S = (g.K + kchunk - 1) / kchunk;
-  SimtSplit sp{(int)S, kchunk, workspace};
+  SimtSplit sp{(int)S, kchunk, workspace, (int64_t)S * g.L * g.M * g.N};
   dim3 grid((unsigned)gm, (unsigned)gn, (unsigned)(g.L * S));
   {
     KernelTimer kt(s, "k_gemm_simt");
@@ -454,9 +461,20 @@ cudaError_t launch_gemm_simt_small_f32(const GemmArgs& g, cudaStream_t s) {
   if (g.M > SimtSmall::BM || g.N > SimtSmall::BN) return cudaErrorNotSupported;
   const int64_t gl = g.L < 65535 ? g.L : 65535;
   KernelTimer kt(s, "k_gemm_simt");
-  k_gemm_simt<AlgF32, SimtSmall><<<dim3(1, 1, (unsigned)gl), 256, 0, s>>>(g, SimtSplit{1, g.K, nullptr});
+  k_gemm_simt<AlgF32, SimtSmall><<<dim3(1, 1, (unsigned)gl), 256, 0, s>>>(g, SimtSplit{1, g.K, nullptr, 0});
   count_launch();
   return cudaGetLastError();
+}
+
+// Read and clear the split-partial self-check flag (0 = no violation).
+int simt_bounds_flag() {
+  int v = 0;
+  if (cudaMemcpyFromSymbol(&v, g_ome_bounds_simt, sizeof(int)) != cudaSuccess) return 0;
+  if (v) {
+    const int zero = 0;
+    cudaMemcpyToSymbol(g_ome_bounds_simt, &zero, sizeof(int));
+  }
+  return v;
 }
 
 cudaError_t launch_gemm_simt_ws(ome_dtype dt, const GemmArgs& g, void* workspace, size_t ws_bytes, int num_sms,

@@ -37,6 +37,15 @@
 namespace ome {
 
 __device__ int g_ome_timeout = 0;
+// First kernel that found an output offset outside its view and skipped the
+// store (self-check of the epilogues; 0 = none); read and cleared by
+// device_status.
+__device__ int g_ome_bounds = 0;
+__device__ __forceinline__ bool in_bounds(int64_t off, int64_t hi, int id) {
+  if (off >= 0 && off <= hi) return true;
+  atomicCAS(&g_ome_bounds, 0, id);
+  return false;
+}
 
 namespace tc {
 constexpr int BM = 128, BN = 128, BK = 32;
@@ -1088,6 +1097,7 @@ struct T2Args {
   GemmArgs g;
   float* partial;                  // [(tiles - F) * S][256][256]
   int TM, TN, NKT, tiles, F, ksplit, units, S;   // all below 2^31 (checked on the host)
+  int64_t c_max, p_max;            // largest element offset of C and of the partials (self-check)
 };
 
 __device__ __forceinline__ uint32_t cluster_rank() {
@@ -1319,7 +1329,6 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(t2::NTHREADS, 1)
   const uint32_t sbase = raw + pad;
   const uint32_t f32_base = sbase;
   const uint32_t term_base = sbase + F32_STAGES * F32_STAGE;
-  float* sums_sm = reinterpret_cast<float*>(smem + F32_STAGES * F32_STAGE + TS * TERM_STAGE);
   uint64_t* bars = reinterpret_cast<uint64_t*>(smem + F32_STAGES * F32_STAGE + TS * TERM_STAGE + Cfg<NT>::SUM_BYTES);
   uint64_t* f32_full = bars;
   uint64_t* f32_empty = f32_full + F32_STAGES;
@@ -1465,6 +1474,9 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(t2::NTHREADS, 1)
       // every MMA must finish before either CTA frees its TMEM
       umma_commit_pair(final_bar, 1);
       mbar_wait_quiesce(final_bar, 0);
+      // and the peer's arrivals on this CTA's drained barrier must have
+      // landed before this CTA's shared memory goes away
+      if (gc >= 1) mbar_wait_quiesce(drained, (gc - 1) & 1);
     }
   } else if (warp < 16) {
     // ---------------- converters + drain + epilogue (warps 0-15) ----------------
@@ -1502,7 +1514,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(t2::NTHREADS, 1)
     bool ok = true;
     auto chunk_end = [&]() -> uint32_t { return dstage + (uint32_t)min((dci + 1) * CHS, unit_stages(du)); };
     auto drain_one = [&]() -> bool {
-      if (!mbar_wait32(sbase + O_CHUNK_DONE, dgc & 1, sbase + O_ABORT)) return false;
+      if (!__all_sync(0xffffffffu, mbar_wait32(sbase + O_CHUNK_DONE, dgc & 1, sbase + O_ABORT))) return false;
       tc_fence_after();
 #pragma unroll
       for (int hh = 0; hh < 8; ++hh) {
@@ -1533,19 +1545,23 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(t2::NTHREADS, 1)
         int dl, dmt, dnt, dkb, dke, dslot;
         decode(du, dl, dmt, dnt, dkb, dke, dslot);
         if (dslot >= 0) {
-          float* pp = t.partial + ((int64_t)dslot * 256 + col0) * 256 + rank * BM + row;
+          const int64_t po = ((int64_t)dslot * 256 + col0) * 256 + rank * BM + row;
+          float* pp = t.partial + po;
+          if (in_bounds(po + 63 * 256, t.p_max, 2))
 #pragma unroll
-          for (int j = 0; j < 64; ++j) pp[(int64_t)j * 256] = j < NSR ? sum[j] : lds32(ssum + (uint32_t)((j - NSR) * NCONV * 4));
+            for (int j = 0; j < 64; ++j)
+              pp[(int64_t)j * 256] = j < NSR ? sum[j] : lds32(ssum + (uint32_t)((j - NSR) * NCONV * 4));
         } else {
           const int64_t m = (int64_t)dmt * 256 + rank * BM + row;
           if (m < g.M) {
             const float sx = scalar_as<float>(g.sx), sy = scalar_as<float>(g.sy);
-            float* crow = static_cast<float*>(g.C) + (g.L > 1 ? (int64_t)dl * g.l_sc[0] : 0) + m * g.m_sc[0];
+            const int64_t roff = (g.L > 1 ? (int64_t)dl * g.l_sc[0] : 0) + m * g.m_sc[0];
+            float* crow = static_cast<float*>(g.C) + roff;
             const int64_t nsc = g.n_sc[0];
             const int n0 = dnt * 256 + col0;
 #pragma unroll
             for (int j = 0; j < 64; ++j) {
-              if (n0 + j < g.N) {
+              if (n0 + j < g.N && in_bounds(roff + (int64_t)(n0 + j) * nsc, t.c_max, 1)) {
                 float* cp = crow + (int64_t)(n0 + j) * nsc;
                 const float v = j < NSR ? sum[j] : lds32(ssum + (uint32_t)((j - NSR) * NCONV * 4));
                 float o = g.sx_one ? v : sx * v;
@@ -1573,8 +1589,13 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(t2::NTHREADS, 1)
         }
         if (!ok) break;
         const int s = it % F32_STAGES, ts = it % TS;
-        if (!mbar_wait32(sbase + O_F32_FULL + 8 * s, (it / F32_STAGES) & 1, sbase + O_ABORT)) { ok = false; break; }
-        if (it >= (uint32_t)TS && !mbar_wait32(sbase + O_TERM_EMPTY + 8 * ts, ((it / TS) - 1) & 1, sbase + O_ABORT)) {
+        // warp-uniform decisions: the warp-synchronous operations below need every lane
+        if (!__all_sync(0xffffffffu, mbar_wait32(sbase + O_F32_FULL + 8 * s, (it / F32_STAGES) & 1, sbase + O_ABORT))) {
+          ok = false;
+          break;
+        }
+        if (it >= (uint32_t)TS &&
+            !__all_sync(0xffffffffu, mbar_wait32(sbase + O_TERM_EMPTY + 8 * ts, ((it / TS) - 1) & 1, sbase + O_ABORT))) {
           ok = false;
           break;
         }
@@ -1591,6 +1612,12 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(t2::NTHREADS, 1)
       }
     }
     while (ok && du < t.units) ok = drain_one();
+    // the multicast commits that free the last term stages arrive on this
+    // CTA's barriers from the leader's tensor core: wait for them to land
+    // before this CTA's shared memory can be reassigned
+    if (tid == 0)
+      for (uint32_t i = it > (uint32_t)TS ? it - TS : 0; i < it; ++i)
+        mbar_wait_quiesce(&term_empty[i % TS], (i / TS) & 1);
   }
   tc_fence_before();
   __syncthreads();
@@ -1618,8 +1645,11 @@ __global__ void __launch_bounds__(256) k_splitk_tiles2(const __grid_constant__ T
     const int64_t m = mt * 256 + mloc, n = nt * 256 + nloc;
     if (m >= g.M || n >= g.N) continue;
     float acc = 0.f;
+    if (!in_bounds(((v * t.S + t.S - 1) * 256 + nloc) * 256 + mloc, t.p_max, 3)) continue;
     for (int s = 0; s < t.S; ++s) acc += t.partial[((v * t.S + s) * 256 + nloc) * 256 + mloc];
-    float* cp = Cp + (g.L > 1 ? l * g.l_sc[0] : 0) + m * g.m_sc[0] + n * g.n_sc[0];
+    const int64_t co = (g.L > 1 ? l * g.l_sc[0] : 0) + m * g.m_sc[0] + n * g.n_sc[0];
+    if (!in_bounds(co, t.c_max, 3)) continue;
+    float* cp = Cp + co;
     float o = g.sx_one ? acc : sx * acc;
     if (!g.sy_zero) o = fmaf(sy, *cp, o);
     *cp = o;
@@ -1750,6 +1780,8 @@ cudaError_t launch_gemm_tma2(const GemmArgs& g, int nterms, void* workspace, siz
   t.S = (int)S;
   t.ksplit = (int)ksplit;
   t.units = (int)units;
+  t.c_max = (g.M - 1) * g.m_sc[0] + (g.N - 1) * g.n_sc[0] + (g.L > 1 ? (g.L - 1) * g.l_sc[0] : 0);
+  t.p_max = (int64_t)(bytes_p / 4) - 1;
   const int grid = (int)(2 * std::min<int64_t>(units, G));
   cudaError_t e;
   {
@@ -1767,6 +1799,304 @@ cudaError_t launch_gemm_tma2(const GemmArgs& g, int nterms, void* workspace, siz
   const int64_t total = Rt * 256 * 256;
   const int64_t nb = (total + 255) / 256;
   k_splitk_tiles2<<<(unsigned)std::min<int64_t>(nb, (int64_t)num_sms * 16), 256, 0, s>>>(t);
+  count_launch();
+  return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// k_gemm_bdiag: batches of small FP32 GEMMs whose batch mode is contiguous in
+// A, B and C (Julia column-major bij,bjk->bik: b fastest), on the tensor
+// cores.
+//
+// Two batches share one 128 x 128 MMA as a block-diagonal product: the A
+// operand stacks A_b (64 rows) over A_b' (64 rows), the B operand stacks
+// B_b^T over B_b'^T, and the diagonal blocks of D are C_b and C_b' (the
+// off-diagonal products are computed and discarded: the kernel is bound by
+// HBM, not by the tensor pipe).  A CTA owns 4 consecutive batches (16 bytes
+// of every (row, k) run, one TMA box of 4 x 64 x 32 per operand and k stage),
+// converts each stage into NT BF16 terms per value in shared memory (the
+// UMMA K-major layout; conflict-free reads and writes), and one thread of
+// warp 8 issues the MMAs of both pairs into main (t0*t0) and cross
+// accumulators (4 x 128 TMEM columns) and the next stage's TMA loads.  The
+// tile leaves through shared memory with the batch mode fastest, as 16-byte
+// stores with the αβ epilogue.  Every wait is bounded.
+namespace bd {
+constexpr int BK = 32, NB = 4;
+constexpr int F32_TILE = NB * 64 * BK * 4;   // one operand, one stage: 32 KB ([k][row][b])
+constexpr int TERM_TILE = 128 * BK * 2;      // one term of one operand of one pair: 8 KB
+constexpr int NCONV = 256, NTHREADS = NCONV + 32;
+constexpr int TMEM_COLS = 512;
+template <int NT> struct Cfg {
+  static constexpr int F32_STAGE = 2 * F32_TILE;                // A, B
+  static constexpr int TERM_BYTES = 2 * 2 * NT * TERM_TILE;     // pairs x operands x terms
+  static constexpr int SMEM_BYTES = 2 * F32_STAGE + TERM_BYTES + 256 + 128;
+};
+}  // namespace bd
+
+static_assert(bd::TERM_TILE == t2::TERM_TILE, "split8_store's term stride");
+
+struct BdArgs {
+  GemmArgs g;
+  int nk;        // k stages of 32
+  int64_t c_max; // largest element offset of C (self-check)
+};
+
+template <int NT>
+__global__ void __launch_bounds__(bd::NTHREADS, 1)
+    k_gemm_bdiag(const __grid_constant__ BdArgs t, const __grid_constant__ CUtensorMap mapA,
+                 const __grid_constant__ CUtensorMap mapB) {
+  using namespace bd;
+  constexpr int F32_STAGE = Cfg<NT>::F32_STAGE;
+  extern __shared__ __align__(128) unsigned char bd_raw[];
+  const uint32_t raw = smem_u32(bd_raw);
+  const uint32_t pad = (128u - (raw & 127u)) & 127u;
+  unsigned char* smem = bd_raw + pad;
+  const uint32_t sbase = raw + pad;
+  const uint32_t f32_base = sbase, term_base = sbase + 2 * F32_STAGE;
+  uint64_t* bars = reinterpret_cast<uint64_t*>(smem + 2 * F32_STAGE + Cfg<NT>::TERM_BYTES);
+  uint64_t* full = bars;            // [2] TMA stage landed
+  uint64_t* conv_done = bars + 2;   // the 8 converter warps wrote a stage's terms
+  uint64_t* mma_done = bars + 3;    // the MMAs of a stage completed
+  uint64_t* final_bar = bars + 4;   // every MMA completed (before TMEM is freed)
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 5);
+  volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
+
+  const GemmArgs& g = t.g;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int b0 = blockIdx.x * NB;
+  if (tid == 0) {
+    mbar_init(&full[0], 1);
+    mbar_init(&full[1], 1);
+    mbar_init(conv_done, 8);
+    mbar_init(mma_done, 1);
+    mbar_init(final_bar, 1);
+    *abort_flag = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 8) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                 "r"(TMEM_COLS)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tmem_slot;
+
+  if (warp == 8) {
+    // ---------------- TMA loads and MMA issue (one thread) ----------------
+    if (lane == 0) {
+      auto load = [&](int c) {
+        const int s = c & 1;
+        mbar_expect_tx(&full[s], 2 * F32_TILE);
+        tma_load_3d(f32_base + s * F32_STAGE, &mapA, b0, 0, c * BK, &full[s]);
+        tma_load_3d(f32_base + s * F32_STAGE + F32_TILE, &mapB, b0, 0, c * BK, &full[s]);
+      };
+      load(0);
+      if (t.nk > 1) load(1);
+      int issued = t.nk > 1 ? 2 : 1;
+      bool ok = true;
+      for (int c = 0; c < t.nk && ok; ++c) {
+        if (!mbar_wait(conv_done, c & 1, abort_flag)) { ok = false; break; }
+        tc_fence_after();
+        // the converters are done with stage c & 1: the stage after next may land there
+        if (c + 2 < t.nk) {
+          load(c + 2);
+          ++issued;
+        }
+#pragma unroll
+        for (int p = 0; p < 2; ++p) {
+          const uint32_t sa = term_base + (uint32_t)((p * 2 + 0) * NT * TERM_TILE);
+          const uint32_t sb = term_base + (uint32_t)((p * 2 + 1) * NT * TERM_TILE);
+          const uint32_t dmain = tmem + 256 * p, dcross = tmem + 256 * p + 128;
+#pragma unroll
+          for (int kk = 0; kk < 2; ++kk) {
+            uint64_t ad[NT], bdsc[NT];
+#pragma unroll
+            for (int q = 0; q < NT; ++q) {
+              ad[q] = umma_desc(sa + q * TERM_TILE + kk * 256);
+              bdsc[q] = umma_desc(sb + q * TERM_TILE + kk * 256);
+            }
+            const uint32_t keep = (c == 0 && kk == 0) ? 0u : 1u;
+            umma_bf16(dmain, ad[0], bdsc[0], keep);
+            bool first_cross = true;
+#pragma unroll
+            for (int d = 1; d < NT; ++d)
+#pragma unroll
+              for (int i = 0; i <= d; ++i) {
+                umma_bf16(dcross, ad[i], bdsc[d - i], first_cross ? keep : 1u);
+                first_cross = false;
+              }
+          }
+        }
+        umma_commit(mma_done);
+      }
+      // every MMA this thread issued must finish before TMEM is freed, and
+      // this CTA's copies in flight must land before it exits
+      umma_commit(final_bar);
+      mbar_wait_quiesce(final_bar, 0);
+      for (int c = issued - 2 > 0 ? issued - 2 : 0; c < issued; ++c) mbar_wait_quiesce(&full[c & 1], (c >> 1) & 1);
+    }
+  } else {
+    // ---------------- converters, then drain and epilogue (warps 0-7) ----------------
+    const int row = tid & 63, c8 = tid >> 6;   // unit (row, 8 k at 8 * c8) of all 4 batches, both operands
+    bool ok = true;
+    for (int c = 0; c < t.nk; ++c) {
+      // warp-uniform decisions: the warp-synchronous operations below need every lane
+      if (!__all_sync(0xffffffffu, mbar_wait(&full[c & 1], (c >> 1) & 1, abort_flag))) { ok = false; break; }
+      if (c > 0 && !__all_sync(0xffffffffu, mbar_wait(mma_done, (c - 1) & 1, abort_flag))) {   // terms free again
+        ok = false;
+        break;
+      }
+#pragma unroll
+      for (int op = 0; op < 2; ++op) {
+        const uint32_t src = f32_base + (c & 1) * F32_STAGE + op * F32_TILE;
+        float v[NB][8];
+#pragma unroll
+        for (int kk = 0; kk < 8; ++kk) {
+          const float4 w = lds128(src + (uint32_t)(((8 * c8 + kk) * 64 + row) * 16));
+          v[0][kk] = w.x;
+          v[1][kk] = w.y;
+          v[2][kk] = w.z;
+          v[3][kk] = w.w;
+        }
+#pragma unroll
+        for (int b = 0; b < NB; ++b) {
+          const int r = (b & 1) * 64 + row;
+          const uint32_t dst = term_base + (uint32_t)((((b >> 1) * 2 + op) * NT) * TERM_TILE) +
+                               (uint32_t)(((r >> 3) * 4 + c8) * 128 + (r & 7) * 16);
+          split8_store<NT>(v[b], dst);   // term stride t2::TERM_TILE == bd::TERM_TILE
+        }
+      }
+      fence_proxy_async();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(conv_done);
+    }
+    // drain: warp w reads TMEM lanes 32 (w & 3).. of pair w >> 2; row r of the
+    // pair's D is batch 2p + (r >> 6), row r & 63; its diagonal block is
+    // columns 64 (r >> 6) ..
+    if (ok) ok = __all_sync(0xffffffffu, mbar_wait(mma_done, (t.nk - 1) & 1, abort_flag));
+    if (ok) {
+      tc_fence_after();
+      const int q = warp & 3, p = warp >> 2;
+      const int r = 32 * q + lane;
+      const int bl = 2 * p + (r >> 6), i = r & 63;
+      const uint32_t lane_off = (uint32_t)(32 * q) << 16;
+      const uint32_t col = (uint32_t)(256 * p + 64 * (r >> 6));
+      // staging [b][n][i] (i fastest) in the first FP32 stage, free by now
+      float* cs = reinterpret_cast<float*>(smem);
+#pragma unroll
+      for (int h = 0; h < 8; ++h) {
+        uint32_t rm[8], rc[8];
+        __syncwarp();
+        tmem_ld8(tmem + lane_off + col + 8 * h, rm);
+        tmem_ld8(tmem + lane_off + col + 128 + 8 * h, rc);
+#pragma unroll
+        for (int j = 0; j < 8; ++j)
+          cs[(bl * 64 + 8 * h + j) * 64 + i] = __uint_as_float(rm[j]) + __uint_as_float(rc[j]);
+      }
+    }
+    tc_fence_before();
+    asm volatile("bar.sync 1, 256;" ::: "memory");   // the 8 converter warps only
+    if (ok) {
+      // 16-byte stores: 4 batches of one (row, column), batch mode fastest
+      const float* cs = reinterpret_cast<const float*>(smem);
+      const float sx = scalar_as<float>(g.sx), sy = scalar_as<float>(g.sy);
+      float* Cp = static_cast<float*>(g.C);
+      const int nb = min(NB, (int)(g.L - b0));
+      for (int e = tid; e < 64 * 64; e += NCONV) {
+        const int i = e & 63, n = e >> 6;
+        if (i >= g.M || n >= g.N) continue;
+        float o[NB];
+#pragma unroll
+        for (int b = 0; b < NB; ++b) {
+          const float v = cs[(b * 64 + n) * 64 + i];
+          o[b] = g.sx_one ? v : sx * v;
+        }
+        const int64_t co = b0 + (int64_t)i * g.m_sc[0] + (int64_t)n * g.n_sc[0];
+        if (!in_bounds(co + nb - 1, t.c_max, 4)) continue;
+        float* cp = Cp + co;
+        if (nb == NB) {
+          if (!g.sy_zero) {
+            const float4 old = *reinterpret_cast<const float4*>(cp);
+            o[0] = fmaf(sy, old.x, o[0]);
+            o[1] = fmaf(sy, old.y, o[1]);
+            o[2] = fmaf(sy, old.z, o[2]);
+            o[3] = fmaf(sy, old.w, o[3]);
+          }
+          *reinterpret_cast<float4*>(cp) = make_float4(o[0], o[1], o[2], o[3]);
+        } else {
+          for (int b = 0; b < nb; ++b) cp[b] = g.sy_zero ? o[b] : fmaf(sy, cp[b], o[b]);
+        }
+      }
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 8) {
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(bd::TMEM_COLS) : "memory");
+  }
+}
+
+namespace {
+// 3-D FP32 tensor map, no swizzle: dims[0] is the contiguous mode; strides in
+// bytes of dims 1 and 2.
+bool make_map3(CUtensorMap* map, const void* base, const cuuint64_t (&dims)[3], const cuuint64_t (&strides)[2],
+               const cuuint32_t (&box)[3]) {
+  EncodeTiledFn fn = encode_fn();
+  if (!fn) return false;
+  cuuint32_t estr[3] = {1, 1, 1};
+  CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, const_cast<void*>(base), dims, strides, box, estr,
+                  CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                  CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS;
+}
+}  // namespace
+
+bool gemm_bdiag_applies(const GemmArgs& g) {
+  if (g.nm != 1 || g.nn != 1 || g.nk != 1 || g.nl != 1) return false;
+  if (g.l_sa[0] != 1 || g.l_sb[0] != 1 || g.l_sc[0] != 1) return false;
+  if (g.M < 1 || g.M > 64 || g.N < 1 || g.N > 64 || g.K < 1 || g.K > 256 || g.L < 4 || g.L >= (1ll << 31))
+    return false;
+  const int64_t st[6] = {g.m_sa[0], g.k_sa[0], g.n_sb[0], g.k_sb[0], g.m_sc[0], g.n_sc[0]};
+  for (int64_t v : st)
+    if (v <= 0 || v % 4 || v >= (1ll << 37)) return false;
+  return !((reinterpret_cast<uintptr_t>(g.A) | reinterpret_cast<uintptr_t>(g.B) | reinterpret_cast<uintptr_t>(g.C)) &
+           15);
+}
+
+cudaError_t launch_gemm_bdiag(const GemmArgs& g, int nterms, cudaStream_t s) {
+  if ((nterms != 2 && nterms != 3) || !gemm_bdiag_applies(g)) return cudaErrorNotSupported;
+  alignas(64) CUtensorMap ma, mb;
+  const cuuint32_t box[3] = {4, 64, 32};
+  const cuuint64_t da[3] = {(cuuint64_t)g.L, (cuuint64_t)g.M, (cuuint64_t)g.K};
+  const cuuint64_t sa[2] = {(cuuint64_t)g.m_sa[0] * 4, (cuuint64_t)g.k_sa[0] * 4};
+  const cuuint64_t db[3] = {(cuuint64_t)g.L, (cuuint64_t)g.N, (cuuint64_t)g.K};
+  const cuuint64_t sb[2] = {(cuuint64_t)g.n_sb[0] * 4, (cuuint64_t)g.k_sb[0] * 4};
+  if (!make_map3(&ma, g.A, da, sa, box) || !make_map3(&mb, g.B, db, sb, box)) return cudaErrorNotSupported;
+  BdArgs t;
+  memset(&t, 0, sizeof(t));
+  t.g = g;
+  t.nk = (int)((g.K + bd::BK - 1) / bd::BK);
+  t.c_max = (g.L - 1) + (g.M - 1) * g.m_sc[0] + (g.N - 1) * g.n_sc[0];
+  const unsigned grid = (unsigned)((g.L + bd::NB - 1) / bd::NB);
+  static bool attr[2] = {false, false};
+  cudaError_t e = cudaSuccess;
+  if (!attr[nterms - 2]) {
+    e = nterms == 3 ? cudaFuncSetAttribute(k_gemm_bdiag<3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           bd::Cfg<3>::SMEM_BYTES)
+                    : cudaFuncSetAttribute(k_gemm_bdiag<2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           bd::Cfg<2>::SMEM_BYTES);
+    if (e != cudaSuccess) return e;
+    attr[nterms - 2] = true;
+  }
+  {
+    KernelTimer kt(s, "k_gemm_bdiag");
+    if (nterms == 3) k_gemm_bdiag<3><<<grid, bd::NTHREADS, bd::Cfg<3>::SMEM_BYTES, s>>>(t, ma, mb);
+    else k_gemm_bdiag<2><<<grid, bd::NTHREADS, bd::Cfg<2>::SMEM_BYTES, s>>>(t, ma, mb);
+  }
   count_launch();
   return cudaGetLastError();
 }
@@ -1804,6 +2134,15 @@ int device_status(cudaStream_t s) {
   if (flag) {
     const int zero = 0;
     cudaMemcpyToSymbol(g_ome_timeout, &zero, sizeof(int));
+  }
+  int bad = 0;
+  e = cudaMemcpyFromSymbol(&bad, g_ome_bounds, sizeof(int));
+  if (e != cudaSuccess) return -(int)e;
+  if (!bad) bad = simt_bounds_flag();
+  if (bad) {
+    const int zero = 0;
+    cudaMemcpyToSymbol(g_ome_bounds, &zero, sizeof(int));
+    return 100 + bad;   // a kernel skipped an out-of-view store (its id)
   }
   return flag;
 }

@@ -104,9 +104,16 @@ size_t gemm_packed_bytes(const GemmArgs& g, int nterms, int num_sms);
 // partials go to `workspace`; cudaErrorNotSupported (nothing launched) when
 // the shape or the workspace does not fit.
 bool gemm_tma2_applies(const GemmArgs& g);
+// Batches of FP32 GEMMs with M, N <= 64, K <= 256 and the batch mode
+// contiguous in A, B and C (column-major bij,bjk->bik) on the tensor cores:
+// two batches per block-diagonal 128 x 128 MMA, four per CTA, operands by TMA.
+bool gemm_bdiag_applies(const GemmArgs& g);
+cudaError_t launch_gemm_bdiag(const GemmArgs& g, int nterms, cudaStream_t s);
 cudaError_t launch_gemm_tma2(const GemmArgs& g, int nterms, void* workspace, size_t ws_bytes, int num_sms,
                              cudaStream_t s);
 
+// Read and clear the CUDA-core GEMM's split-partial self-check flag.
+int simt_bounds_flag();
 // Synchronise s and read/clear the device timeout flag: 1 if a bounded wait
 // gave up, 0 if not, -cudaError on failure.
 int device_status(cudaStream_t s);

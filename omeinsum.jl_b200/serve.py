@@ -7,9 +7,12 @@ fixed number of slots; each slot owns a CUDA stream, a host thread that
 issues its job, and a library context whose device workspace (the slot's
 share of the HBM budget) holds one job's intermediates.  Jobs are admitted in
 arrival order when a slot is free and the job's planned peak workspace bytes
-(``ome_plan_peak_bytes``) fit a slot's share; larger jobs are rejected; their
-work overlaps on the device (one stream per slot, the slices of different
-jobs interleave); a finished slot takes the next job at once.  Latency is
+(``ome_plan_peak_bytes``) fit a slot's share; a job larger than a share but
+within the whole budget (a gradient job keeps every intermediate) waits until
+the device is idle and runs alone in a workspace of its own size; only jobs
+beyond the budget are rejected.  Work of different jobs overlaps on the
+device (one stream per slot, the slices of different jobs interleave); a
+finished slot takes the next job at once.  Latency is
 measured from arrival to the completion event of the job's last kernel.
 
 Large networks: ``pow2_rescale`` scales every input by an exact power of two
@@ -59,7 +62,7 @@ def pow2_rescale(xs: Sequence[Any]):
     return out, exps
 
 
-@dataclass
+@dataclass(eq=False)   # jobs compare by identity (they hold tensors)
 class Job:
     code: Any
     xs: List[torch.Tensor]
@@ -75,6 +78,8 @@ class Job:
     _event: Any = None
     _slot: int = -1
     _bytes: int = 0
+    _work: Optional[float] = None
+    reject_reason: str = ""       # "memory" (beyond the budget) or "work" (beyond max_job_flops)
 
     def scalar(self) -> float:
         """The contraction value as a Python float (mantissa * 2^log2_scale)."""
@@ -93,6 +98,7 @@ class _Slot:
         self.device = device
         self.stream = torch.cuda.Stream(device=device)
         self.ctx: Optional[_lib.Context] = None
+        self.exclusive = False   # the context is a one-job workspace beyond a slot's share
         self.job: Optional[Job] = None
         self.issued = threading.Event()
         self.error: Optional[BaseException] = None
@@ -118,8 +124,15 @@ class TNServer:
     slot's first job and kept until close(): freeing device memory
     synchronises the whole device, which would stall every running job."""
 
-    def __init__(self, n_slots: int = 8, hbm_budget_bytes: float = 150e9, device: int = 0, prec: int = 0):
+    def __init__(self, n_slots: int = 8, hbm_budget_bytes: float = 150e9, device: int = 0, prec: int = 0,
+                 max_job_flops: Optional[float] = None):
+        """``max_job_flops`` (optional): jobs whose contraction tree needs more
+        multiply-adds than this (the planner's time complexity, gradient jobs
+        counted as three forward passes) are rejected at admission, as a
+        service would refuse work that holds the device for minutes; None
+        admits everything that fits the memory budget."""
         self.device = torch.device("cuda", device)
+        self.max_job_flops = max_job_flops
         self.slots = [_Slot(self.device) for _ in range(n_slots)]
         self.budget = int(hbm_budget_bytes)
         self.slot_bytes = int(hbm_budget_bytes) // n_slots
@@ -153,6 +166,14 @@ class TNServer:
         need = plan.grad_bytes if job.grad else plan.forward_bytes
         return p, [_f_contig(t) for t in ts], sd, plan, need
 
+    def _work(self, job: Job) -> float:
+        """Multiply-adds of the job's tree (gradient jobs: three forward passes)."""
+        if job._work is None:
+            from .planner import contraction_complexity
+            sd = get_size_dict(job.code.getixsv(), job.xs)
+            job._work = 2.0 ** contraction_complexity(job.code, sd).tc * (3.0 if job.grad else 1.0)
+        return job._work
+
     def _launch(self, slot: _Slot, job: Job, prepared):
         """Reserve the slot and hand the job's kernel issue to the slot's thread."""
         p, ins, sd, plan, need = prepared
@@ -165,6 +186,21 @@ class TNServer:
         slot.issued.clear()
         slot.error = None
         slot.work.put(lambda: self._issue(slot, job, prepared))
+
+    def _launch_exclusive(self, job: Job, prepared):
+        """Run one job that exceeds a slot's share: all slot workspaces are
+        released, slot 0 gets a context of the job's planned peak bytes, and
+        the job runs alone; the context is released when the job retires."""
+        need = prepared[4]
+        torch.cuda.synchronize(self.device)
+        for s in self.slots:
+            if s.ctx is not None:
+                s.ctx.close()
+                s.ctx = None
+        slot = self.slots[0]
+        slot.ctx = _lib.Context(self.device.index, need)   # MemoryError -> caller
+        slot.exclusive = True
+        self._launch(slot, job, prepared)
 
     def _issue(self, slot: _Slot, job: Job, prepared):
         p, ins, sd, plan, need = prepared
@@ -205,6 +241,11 @@ class TNServer:
                 s.job.done = self.clock()
                 self.rejected.append(s.job)
                 s.job = None
+                if s.exclusive:
+                    s.stream.synchronize()
+                    s.ctx.close()
+                    s.ctx = None
+                    s.exclusive = False
                 if not isinstance(err, MemoryError):
                     raise err
                 continue
@@ -213,23 +254,45 @@ class TNServer:
                 s.job.done = now
                 self.finished.append(s.job)
                 s.job = None
+                if s.exclusive:
+                    s.ctx.close()   # the job has finished: the workspace is free
+                    s.ctx = None
+                    s.exclusive = False
         while self.queue:
             free = [s for s in self.slots if s.job is None]
             if not free:
                 break
             job = self.queue[0]
+            if self.max_job_flops is not None and self._work(job) > self.max_job_flops:
+                self.queue.popleft()
+                job.done = self.clock()
+                job.reject_reason = "work"
+                self.rejected.append(job)
+                continue
             prepared = self._plan(job)
             need = prepared[4]
             if need > self.budget:
                 self.queue.popleft()
                 job.done = self.clock()
+                job.reject_reason = "memory"
                 self.rejected.append(job)
                 continue
             running = any(s.job is not None for s in self.slots)
             if need > self.slot_bytes:
-                self.queue.popleft()  # larger than a slot's share of the budget: never admitted
-                job.done = self.clock()
-                self.rejected.append(job)
+                # larger than a slot's share (typically a gradient job, which
+                # keeps every intermediate): it waits, in arrival order, until
+                # the device is idle, then runs alone in a workspace of its own
+                # size taken from the whole budget; the slots' workspaces are
+                # released first (freeing memory synchronises the device, which
+                # costs nothing once it is idle)
+                if running:
+                    break
+                self.queue.popleft()
+                try:
+                    self._launch_exclusive(job, prepared)
+                except MemoryError:
+                    job.done = self.clock()
+                    self.rejected.append(job)
                 continue
             slot = next((s for s in free if s.ctx is not None), free[0])
             if slot.ctx is None and self.slot_bytes + (256 << 20) > torch.cuda.mem_get_info(self.device)[0]:
@@ -268,18 +331,28 @@ class TNServer:
         return self.stats()
 
     def close(self):
-        """Stop the slot threads and free every slot's workspace."""
+        """Stop the slot threads and free every slot's workspace; a job error
+        that no poll() has reported yet is raised here."""
+        pending = None
         for s in self.slots:
             s.work.put(None)
-            s.thread.join(timeout=60)
+            # no timeout: a slot thread may still be issuing a job's kernels,
+            # and its workspace must not be freed under them
+            s.thread.join()
+            if s.error is not None and pending is None:
+                pending = s.error
+        for s in self.slots:
             s.stream.synchronize()
             if s.ctx is not None:
                 s.ctx.close()
                 s.ctx = None
+        if pending is not None:
+            raise pending
 
     def stats(self):
         lat = np.array([j.latency for j in self.finished]) if self.finished else np.zeros(1)
         span = max((j.done for j in self.finished), default=0.0) - min((j.arrival for j in self.finished), default=0.0)
         return {"completed": len(self.finished), "rejected": len(self.rejected),
+                "rejected_over_work_cap": sum(1 for j in self.rejected if j.reject_reason == "work"),
                 "p50_ms": float(np.percentile(lat, 50) * 1e3), "p99_ms": float(np.percentile(lat, 99) * 1e3),
                 "jobs_per_s": len(self.finished) / span if span > 0 else 0.0, "makespan_s": span}

@@ -34,7 +34,7 @@ pytestmark = pytest.mark.gpu
 MAIN_KERNEL = {
     "abcd,cdef->abef": ("k_gemm_tma2", "k_gemm_simt"),
     "ijk,jkl->il": ("k_gemm_tma2", "k_gemm_simt"),
-    "bij,bjk->bik": ("k_gemm_bstage", "k_gemm_bstage"),
+    "bij,bjk->bik": ("k_gemm_bdiag", "k_gemm_bstage"),
     "abcde->ecadb": ("k_transpose_v4", "k_transpose32"),
     "ii->": ("k_loop_block", "k_loop_block"),
     "ijk->j": ("k_reduce_contig", "k_reduce_contig"),

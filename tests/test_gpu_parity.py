@@ -463,3 +463,34 @@ def test_cuda_core_gemm_split_k(code, sizes, dt):
             assert_match(to_np(yd), 2 * oracle(ixs, iy, xs, sizes, dt) + 3 * y0, dt)
     finally:
         ome.set_einsum_backend(ome.B200Backend())
+
+
+@pytest.mark.parametrize("prec,rtol", [(3, 1e-6), (2, 1e-5)])
+@pytest.mark.parametrize("code,sizes", [
+    ("bij,bjk->bik", dict(b=512, i=64, j=64, k=64)),    # the benchmark's shape: whole boxes
+    ("bij,bjk->bik", dict(b=100, i=37, j=50, k=23)),    # ragged rows, columns and k, a last group of 4
+    ("bij,bkj->bki", dict(b=64, i=64, j=200, k=48)),    # B and C with transposed modes, 7 k stages
+    ("bij,bjk->bik", dict(b=8, i=16, j=8, k=64)),       # one k stage, mostly padding
+])
+def test_batch_innermost_tensor_core_gemm(code, sizes, prec, rtol):
+    """Batches of small FP32 GEMMs with the batch mode contiguous everywhere
+    (column-major bij,bjk->bik) on the tensor cores, two batches per
+    block-diagonal MMA, against FP64, with y <- 2y + 3f on a second call."""
+    rng = np.random.default_rng(43)
+    ixs, iy = parse(code)
+    xs = [gen(rng, [sizes[l] for l in ix], "f32") for ix in ixs]
+    c = ome.EinCode(ixs, iy)
+    dxs = [to_dev(x, "f32") for x in xs]
+    want = oracle(ixs, iy, xs, sizes, "f32", wide=True)
+    ome.set_einsum_backend(ome.B200Backend(prec=prec))
+    try:
+        got, names = kernel_names(lambda: ome.einsum(c, dxs, sizes))
+        assert names == ["k_gemm_bdiag"], names
+        assert_match(to_np(got), want, "f32", rtol)
+        y0 = gen(rng, [sizes[l] for l in iy], "f32")
+        yd = to_dev(y0, "f32")
+        ome.einsum_(c, dxs, yd, 3, 2, sizes)
+        ome.device_status()
+        assert_match(to_np(yd), 3 * want + 2 * y0.astype(np.float64), "f32", rtol)
+    finally:
+        ome.set_einsum_backend(ome.B200Backend())
