@@ -1824,7 +1824,7 @@ namespace bd {
 constexpr int BK = 32, NB = 4;
 constexpr int F32_TILE = NB * 64 * BK * 4;   // one operand, one stage: 32 KB ([k][row][b])
 constexpr int TERM_TILE = 128 * BK * 2;      // one term of one operand of one pair: 8 KB
-constexpr int NCONV = 256, NTHREADS = NCONV + 32;
+constexpr int NCONV = 512, NTHREADS = NCONV + 32;   // converter warps 0-15, control warp 16
 constexpr int TMEM_COLS = 512;
 template <int NT> struct Cfg {
   static constexpr int F32_STAGE = 2 * F32_TILE;                // A, B
@@ -1867,13 +1867,13 @@ __global__ void __launch_bounds__(bd::NTHREADS, 1)
   if (tid == 0) {
     mbar_init(&full[0], 1);
     mbar_init(&full[1], 1);
-    mbar_init(conv_done, 8);
+    mbar_init(conv_done, 16);
     mbar_init(mma_done, 1);
     mbar_init(final_bar, 1);
     *abort_flag = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
-  if (warp == 8) {
+  if (warp == 16) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
                  "r"(TMEM_COLS)
                  : "memory");
@@ -1884,7 +1884,7 @@ __global__ void __launch_bounds__(bd::NTHREADS, 1)
   tc_fence_after();
   const uint32_t tmem = *tmem_slot;
 
-  if (warp == 8) {
+  if (warp == 16) {
     // ---------------- TMA loads and MMA issue (one thread) ----------------
     if (lane == 0) {
       auto load = [&](int c) {
@@ -1939,8 +1939,9 @@ __global__ void __launch_bounds__(bd::NTHREADS, 1)
       for (int c = issued - 2 > 0 ? issued - 2 : 0; c < issued; ++c) mbar_wait_quiesce(&full[c & 1], (c >> 1) & 1);
     }
   } else {
-    // ---------------- converters, then drain and epilogue (warps 0-7) ----------------
-    const int row = tid & 63, c8 = tid >> 6;   // unit (row, 8 k at 8 * c8) of all 4 batches, both operands
+    // ---------------- converters, then drain and epilogue (warps 0-15) ----------------
+    // unit (row, 8 k at 8 * c8) of all 4 batches of operand op
+    const int row = tid & 63, c8 = (tid >> 6) & 3, op = tid >> 8;
     bool ok = true;
     for (int c = 0; c < t.nk; ++c) {
       // warp-uniform decisions: the warp-synchronous operations below need every lane
@@ -1949,8 +1950,7 @@ __global__ void __launch_bounds__(bd::NTHREADS, 1)
         ok = false;
         break;
       }
-#pragma unroll
-      for (int op = 0; op < 2; ++op) {
+      {
         const uint32_t src = f32_base + (c & 1) * F32_STAGE + op * F32_TILE;
         float v[NB][8];
 #pragma unroll
@@ -1973,32 +1973,32 @@ __global__ void __launch_bounds__(bd::NTHREADS, 1)
       __syncwarp();
       if (lane == 0) mbar_arrive(conv_done);
     }
-    // drain: warp w reads TMEM lanes 32 (w & 3).. of pair w >> 2; row r of the
-    // pair's D is batch 2p + (r >> 6), row r & 63; its diagonal block is
-    // columns 64 (r >> 6) ..
+    // drain: warp w reads TMEM lanes 32 (w & 3).. of pair (w >> 2) & 1, 32 of
+    // the columns (half w >> 3); row r of the pair's D is batch 2p + (r >> 6),
+    // row r & 63; its diagonal block is columns 64 (r >> 6) ..
     if (ok) ok = __all_sync(0xffffffffu, mbar_wait(mma_done, (t.nk - 1) & 1, abort_flag));
     if (ok) {
       tc_fence_after();
-      const int q = warp & 3, p = warp >> 2;
+      const int q = warp & 3, p = (warp >> 2) & 1, ch = warp >> 3;
       const int r = 32 * q + lane;
       const int bl = 2 * p + (r >> 6), i = r & 63;
       const uint32_t lane_off = (uint32_t)(32 * q) << 16;
-      const uint32_t col = (uint32_t)(256 * p + 64 * (r >> 6));
+      const uint32_t col = (uint32_t)(256 * p + 64 * (r >> 6) + 32 * ch);
       // staging [b][n][i] (i fastest) in the first FP32 stage, free by now
       float* cs = reinterpret_cast<float*>(smem);
 #pragma unroll
-      for (int h = 0; h < 8; ++h) {
+      for (int h = 0; h < 4; ++h) {
         uint32_t rm[8], rc[8];
         __syncwarp();
         tmem_ld8(tmem + lane_off + col + 8 * h, rm);
         tmem_ld8(tmem + lane_off + col + 128 + 8 * h, rc);
 #pragma unroll
         for (int j = 0; j < 8; ++j)
-          cs[(bl * 64 + 8 * h + j) * 64 + i] = __uint_as_float(rm[j]) + __uint_as_float(rc[j]);
+          cs[(bl * 64 + 32 * ch + 8 * h + j) * 64 + i] = __uint_as_float(rm[j]) + __uint_as_float(rc[j]);
       }
     }
     tc_fence_before();
-    asm volatile("bar.sync 1, 256;" ::: "memory");   // the 8 converter warps only
+    asm volatile("bar.sync 1, 512;" ::: "memory");   // the 16 converter warps only
     if (ok) {
       // 16-byte stores: 4 batches of one (row, column), batch mode fastest
       const float* cs = reinterpret_cast<const float*>(smem);
@@ -2034,7 +2034,7 @@ __global__ void __launch_bounds__(bd::NTHREADS, 1)
   }
   tc_fence_before();
   __syncthreads();
-  if (warp == 8) {
+  if (warp == 16) {
     tc_fence_after();
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(bd::TMEM_COLS) : "memory");
   }
