@@ -283,7 +283,7 @@ OME_API int ome_slice_greedy(int32_t ntensors, const int32_t* nlabels, const int
  * (outer1, outer2, inner, batch) each merge into one strided mode -- e.g.
  * every contraction of an MPS sweep.  ome_batch_create analyses them like
  * ome_einsum does (src/einsum.jl:139-211), uploads a problem table, and times
- * the candidate tile shapes on the batch (tile_config < 0; or pick 0..2);
+ * the candidate kernels on the batch (tile_config < 0; or pick 0..3);
  * ome_batch_run issues ONE persistent grouped kernel over all problems' tiles
  * (capturable in a CUDA graph).  Tensors are bound at creation: the buffers
  * must stay valid.  Replaces a loop of einsum! calls, one launch each. */
@@ -292,7 +292,10 @@ OME_API int ome_batch_create(ome_ctx* ctx, void* stream, ome_dtype dtype, int32_
                              const ome_tensor* x1s, const ome_tensor* x2s, const ome_tensor* ys,
                              int32_t tile_config, ome_batch** out);
 OME_API int ome_batch_run(ome_ctx* ctx, ome_batch* batch, void* stream, const void* sx, const void* sy);
-/* Chosen tile shape (0: 32x32, 1: 64x32, 2: 64x64) and the autotuner's timings (us, 3 floats). */
+/* Chosen kernel (0: 32x32, 1: 64x32, 2: 64x64 CUDA-core tiles; 3: the tensor-core
+ * grouped kernel, 128 x 128 tiles of BF16x6 split products, F32 and C32 only --
+ * C32 as the real 2 x 2 embedding) and the autotuner's timings (us, 4 floats;
+ * -1 for a kernel that is not a candidate for the dtype). */
 OME_API int ome_batch_info(const ome_batch* batch, int32_t* tile_config, float* tuned_us);
 OME_API int ome_batch_destroy(ome_batch* batch);
 

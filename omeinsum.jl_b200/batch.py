@@ -67,7 +67,7 @@ class BatchedEinsum:
                                                int(tile_config), C.byref(h)))
         self.handle = h
         cfg = C.c_int32()
-        us = (C.c_float * 3)()
+        us = (C.c_float * 4)()
         check(_lib.load().ome_batch_info(h, C.byref(cfg), us))
         self.tile_config = cfg.value
         self.tuned_us = list(us)

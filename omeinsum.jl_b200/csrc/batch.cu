@@ -17,18 +17,6 @@
 
 namespace ome {
 
-struct GroupProblem {
-  const void* a;
-  const void* b;
-  void* c;
-  int64_t m, n, k, l;
-  int64_t a_sm, a_sk, a_sl;
-  int64_t b_sk, b_sn, b_sl;
-  int64_t c_sm, c_sn, c_sl;
-  int64_t tile_begin;  // first global tile index of this problem
-  int32_t tiles_m, tiles_n;
-};
-
 template <int BM, int BN, int TM, int TN>
 struct GroupCfg {
   static constexpr int NT = (BM / TM) * (BN / TN);
@@ -110,9 +98,13 @@ __global__ void __launch_bounds__((BM / TM) * (BN / TN)) k_group_gemm(const Grou
   }
 }
 
-// candidate tile shapes (BM, BN, TM, TN)
-constexpr int NCFG = 3;
-static const int kCfg[NCFG][4] = {{32, 32, 2, 2}, {64, 32, 4, 2}, {64, 64, 4, 4}};
+// candidate tile shapes (BM, BN, TM, TN) of the CUDA-core kernel, then the
+// tensor-core kernel (k_group_tc, 128 x 128 tiles of the real-embedded
+// output; F32 and C32 only)
+constexpr int NCFG = 4, CFG_TC = 3;
+static const int kCfg[NCFG][4] = {{32, 32, 2, 2}, {64, 32, 4, 2}, {64, 64, 4, 4}, {128, 128, 0, 0}};
+
+static bool tc_dtype(ome_dtype dt) { return dt == OME_F32 || dt == OME_C32; }
 
 template <class A>
 static cudaError_t launch_group_t(int cfg, const GroupProblem* d, int n, int64_t tiles, int grid, const Scalar& sx,
@@ -137,10 +129,19 @@ struct ome_batch {
   int device;
   int num_sms;
   std::vector<GroupProblem> host[NCFG];   // per tile shape (tile_begin differs)
-  GroupProblem* dev[NCFG] = {nullptr, nullptr, nullptr};
-  int64_t tiles[NCFG] = {0, 0, 0};
-  float tuned_us[NCFG] = {0, 0, 0};
+  GroupProblem* dev[NCFG] = {nullptr, nullptr, nullptr, nullptr};
+  int64_t tiles[NCFG] = {0, 0, 0, 0};
+  float tuned_us[NCFG] = {0, 0, 0, 0};
+  std::vector<int32_t> tile_prob_host;     // tensor-core tiles: owning problem of each tile
+  int32_t* tile_prob = nullptr;
 };
+
+static void free_batch(ome_batch* b) {
+  for (int c = 0; c < NCFG; ++c)
+    if (b->dev[c]) cudaFree(b->dev[c]);
+  if (b->tile_prob) cudaFree(b->tile_prob);
+  delete b;
+}
 
 namespace {
 
@@ -207,11 +208,23 @@ int to_problem(const HView& x1v, const HView& x2v, const HView& yv, GroupProblem
   return OME_OK;
 }
 
+// 1 when an operand's K mode is contiguous and every row it reads starts on
+// 16 bytes (per16 elements per 16 bytes).
+int32_t kvec_ok(const void* base, int64_t sk, int64_t s_row, int64_t rows, int64_t s_l, int64_t l, int per16) {
+  if (sk != 1 || (reinterpret_cast<uintptr_t>(base) & 15u) != 0) return 0;
+  if (rows > 1 && s_row % per16 != 0) return 0;
+  if (l > 1 && s_l % per16 != 0) return 0;
+  return 1;
+}
+
 cudaError_t launch_cfg(ome_batch* b, int cfg, const Scalar& sx, const Scalar& sy, cudaStream_t s) {
   const int64_t tiles = b->tiles[cfg];
   if (tiles == 0) return cudaSuccess;
   const int grid = (int)std::min<int64_t>(tiles, (int64_t)b->num_sms * 8);
   const int syz = scalar_is_zero(b->dt, sy), sxo = scalar_is_one(b->dt, sx);
+  if (cfg == CFG_TC)
+    return launch_group_tc(b->dt, 3, b->dev[cfg], b->tile_prob, b->nprob, tiles,
+                           (int)std::min<int64_t>(tiles, b->num_sms), sx, sy, syz, sxo, s);
   cudaError_t e = cudaErrorInvalidValue;
   OME_DISPATCH(b->dt, ALG, e = launch_group_t<ALG>(cfg, b->dev[cfg], b->nprob, tiles, grid, sx, sy, syz, sxo, s));
   return e;
@@ -242,12 +255,21 @@ int ome_batch_create(ome_ctx* ctx, void* stream, ome_dtype dtype, int32_t count,
       delete b;
       return rc;
     }
+    GroupProblem& p = probs[i];
+    const int per16 = dtype == OME_C32 ? 2 : 4;
+    p.a_kvec = p.b_kvec = 0;
+    if (tc_dtype(dtype)) {
+      p.a_kvec = kvec_ok(p.a, p.a_sk, p.a_sm, p.m, p.a_sl, p.l, per16);
+      p.b_kvec = kvec_ok(p.b, p.b_sk, p.b_sn, p.n, p.b_sl, p.l, per16);
+    }
   }
   for (int c = 0; c < NCFG; ++c) {
     b->host[c] = probs;
     int64_t t = 0;
     for (auto& p : b->host[c]) {
-      p.tiles_m = (int32_t)((p.m + kCfg[c][0] - 1) / kCfg[c][0]);
+      // the tensor-core tiles count rows of the real embedding (two per complex row)
+      const int64_t rows = c == CFG_TC && dtype == OME_C32 ? 2 * p.m : p.m;
+      p.tiles_m = (int32_t)((rows + kCfg[c][0] - 1) / kCfg[c][0]);
       p.tiles_n = (int32_t)((p.n + kCfg[c][1] - 1) / kCfg[c][1]);
       p.tile_begin = t;
       t += (int64_t)p.tiles_m * p.tiles_n * p.l;
@@ -257,14 +279,28 @@ int ome_batch_create(ome_ctx* ctx, void* stream, ome_dtype dtype, int32_t count,
     if (e == cudaSuccess)
       e = cudaMemcpyAsync(b->dev[c], b->host[c].data(), sizeof(GroupProblem) * (size_t)count,
                           cudaMemcpyHostToDevice, static_cast<cudaStream_t>(stream));
+    if (e == cudaSuccess && c == CFG_TC && tc_dtype(dtype)) {
+      b->tile_prob_host.resize((size_t)t);
+      for (int i = 0; i < count; ++i) {
+        const GroupProblem& p = b->host[c][i];
+        const int64_t n = (int64_t)p.tiles_m * p.tiles_n * p.l;
+        std::fill_n(b->tile_prob_host.begin() + p.tile_begin, n, (int32_t)i);
+      }
+      e = cudaMalloc(&b->tile_prob, sizeof(int32_t) * std::max<size_t>((size_t)t, 1));
+      if (e == cudaSuccess && t > 0)
+        e = cudaMemcpyAsync(b->tile_prob, b->tile_prob_host.data(), sizeof(int32_t) * (size_t)t,
+                            cudaMemcpyHostToDevice, static_cast<cudaStream_t>(stream));
+    }
     if (e != cudaSuccess) {
-      for (int q = 0; q <= c; ++q)
-        if (b->dev[q]) cudaFree(b->dev[q]);
-      delete b;
+      free_batch(b);
       return cuda_err(e, "batch table");
     }
   }
   cudaStream_t s = static_cast<cudaStream_t>(stream);
+  if (tile_config == CFG_TC && !tc_dtype(dtype)) {
+    free_batch(b);
+    return set_err(OME_UNSUPPORTED, "the tensor-core grouped launch takes Float32 and ComplexF32 only");
+  }
   if (tile_config >= 0 && tile_config < NCFG) {
     b->cfg = tile_config;
   } else {
@@ -276,6 +312,10 @@ int ome_batch_create(ome_ctx* ctx, void* stream, ome_dtype dtype, int32_t count,
     float best = 1e30f;
     b->cfg = NCFG - 1;
     for (int c = 0; c < NCFG; ++c) {
+      if (c == CFG_TC && !tc_dtype(dtype)) {
+        b->tuned_us[c] = -1.f;   // not a candidate for this dtype
+        continue;
+      }
       launch_cfg(b, c, one, zero, s);  // warm-up
       cudaEventRecord(e0, s);
       for (int r = 0; r < 3; ++r) launch_cfg(b, c, one, zero, s);
@@ -293,8 +333,7 @@ int ome_batch_create(ome_ctx* ctx, void* stream, ome_dtype dtype, int32_t count,
     cudaEventDestroy(e1);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) {
-      for (int q = 0; q < NCFG; ++q) cudaFree(b->dev[q]);
-      delete b;
+      free_batch(b);
       return cuda_err(e, "batch autotune");
     }
   }
@@ -319,9 +358,7 @@ int ome_batch_info(const ome_batch* b, int32_t* tile_config, float* tuned_us) {
 
 int ome_batch_destroy(ome_batch* b) {
   if (!b) return OME_OK;
-  for (int c = 0; c < NCFG; ++c)
-    if (b->dev[c]) cudaFree(b->dev[c]);
-  delete b;
+  free_batch(b);
   return OME_OK;
 }
 

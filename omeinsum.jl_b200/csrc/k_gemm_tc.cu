@@ -2101,6 +2101,642 @@ cudaError_t launch_gemm_bdiag(const GemmArgs& g, int nterms, cudaStream_t s) {
   return cudaGetLastError();
 }
 
+// ---------------------------------------------------------------------------
+// k_group_tc: one persistent launch over the tiles of many uneven binary
+// contractions (a grouped GEMM: the MPS transfer contractions of a sweep), on
+// the tensor cores.
+//
+// Complex64 problems run as real GEMMs of their 2 x 2 embedding: with
+// A' [(m, p), (k, q)] = (q == p ? Re A : (p == 0 ? -Im A : Im A))[m, k] and
+// B' [(k, q), n] = (q == 0 ? Re B : Im B)[k, n], C' = A' B' holds
+// C'[(m, 0), n] = Re C[m, n] and C'[(m, 1), n] = Im C[m, n] -- four real
+// products per complex one, as many as the four real GEMMs, and C' is C's own
+// interleaved storage.
+//
+// Warp roles (14 warps, one CTA per SM):
+//   13     scheduler: walks this CTA's tiles (tile = blockIdx.x + j gridDim.x),
+//          looks up each tile's problem in a host-built tile -> problem table
+//          and stages the problem's descriptor and the tile's (l, m, n)
+//          coordinates in a ring of shared-memory slots;
+//   0-7    converters: load each 32-wide (real) k stage of a tile's A' and B'
+//          straight from the strided inputs (the next stage's loads are in
+//          flight while the current one is split), split it into NT BF16
+//          terms and store them in the UMMA K-major layout;
+//   12     MMA issue (lane 0): main and cross-term accumulators, two TMEM
+//          buffers, a fresh accumulation every CHUNK stages;
+//   8-11   drain (one warp per TMEM lane quarter): each finished chunk into FP32 running sums in shared
+//          memory; the tile's last chunk goes straight from TMEM through the
+//          alpha-beta epilogue to the output (complex: the two parts of an
+//          element are neighbouring lanes).
+// A tile's drain and epilogue overlap the next tile's loads and MMAs.  Every
+// wait is bounded.
+namespace gt {
+constexpr int BM = 128, BN = 128, BK = 32, CHUNK = 8;
+constexpr int TILE_BYTES = BM * BK * 2;      // one term of one operand, one stage: 8 KB
+constexpr int NTHREADS = 14 * 32;            // at most 4 warps per SM quarter: 128 registers a thread
+constexpr int ACC_BYTES = BM * BN * 4;
+constexpr int TMEM_COLS = 512;
+constexpr int NSLOT = 8;                     // scheduler ring
+constexpr int SLOT_BYTES = 192;
+constexpr int SLOT_USERS = 13;               // 8 converter warps + 4 drain warps + the MMA thread
+template <int NT> struct Cfg {
+  static constexpr int STAGE_BYTES = 2 * NT * TILE_BYTES;
+  static constexpr int STAGES = NT == 2 ? 4 : 3;
+  static constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + ACC_BYTES + NSLOT * SLOT_BYTES + 512 + 128;
+};
+}  // namespace gt
+
+// One staged tile: its problem and the tile's coordinates.
+struct __align__(16) GtTile {
+  GroupProblem p;
+  int64_t li, mt, nt;
+};
+static_assert(sizeof(GtTile) <= gt::SLOT_BYTES, "scheduler slot");
+static_assert(sizeof(GroupProblem) % 8 == 0 && sizeof(GroupProblem) / 8 <= 32, "descriptor copy by one warp");
+
+struct GtArgs {
+  const GroupProblem* probs;
+  const int32_t* tile_prob;   // [tiles] owning problem of each global tile
+  int nprob;
+  int64_t tiles;
+  Scalar sx, sy;
+  int sy_zero, sx_one;
+};
+
+template <bool CPLX>
+__device__ __forceinline__ int gt_stages(const GroupProblem& p) {
+  const int64_t kr = CPLX ? 2 * p.k : p.k;   // real K of the (embedded) GEMM
+  return (int)((kr + gt::BK - 1) / gt::BK);
+}
+
+static_assert(gt::TILE_BYTES == t2::TERM_TILE, "split8_store's term stride");
+
+__device__ __forceinline__ void tmem_ld16_nw(uint32_t taddr, uint32_t (&r)[16]) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
+      "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr));
+}
+__device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+
+// Scheduler warp: stage every tile of this CTA, in order, in the slot ring.
+__device__ __forceinline__ void gt_scheduler(const GtArgs& t, unsigned char* slots, uint64_t* sched_full,
+                                             uint64_t* sched_empty, volatile int* abort_flag, int lane) {
+  using namespace gt;
+  uint32_t j = 0;
+  for (int64_t tile = blockIdx.x; tile < t.tiles; tile += gridDim.x, ++j) {
+    const int s = j % NSLOT;
+    if (j >= (uint32_t)NSLOT &&
+        !__all_sync(0xffffffffu, mbar_wait(&sched_empty[s], ((j / NSLOT) - 1) & 1, abort_flag)))
+      return;
+    const int pi = __ldg(t.tile_prob + tile);
+    bool bad = pi < 0 || pi >= t.nprob;
+    int64_t r = 0, tm = 1, per_l = 1;
+    if (!bad) {
+      const GroupProblem& p = t.probs[pi];
+      r = tile - __ldg(&p.tile_begin);
+      tm = __ldg(&p.tiles_m);
+      per_l = tm * __ldg(&p.tiles_n);
+      bad = per_l <= 0 || r < 0 || r >= per_l * __ldg(&p.l);
+    }
+    if (bad) {   // a table that does not match the problems: record it and stop
+      if (lane == 0) {
+        atomicCAS(&g_ome_bounds, 0, 5);
+        *abort_flag = 1;
+      }
+      return;
+    }
+    GtTile* ti = reinterpret_cast<GtTile*>(slots + s * SLOT_BYTES);
+    const uint64_t* src = reinterpret_cast<const uint64_t*>(t.probs + pi);
+    if (lane < (int)(sizeof(GroupProblem) / 8)) reinterpret_cast<uint64_t*>(&ti->p)[lane] = __ldg(src + lane);
+    if (lane == 0) {
+      const int64_t li = r / per_l;
+      r -= li * per_l;
+      ti->li = li;
+      ti->mt = r % tm;
+      ti->nt = r / tm;
+    }
+    __syncwarp();
+    if (lane == 0) mbar_arrive(&sched_full[s]);
+  }
+}
+
+// One converter thread's share of one stage, in registers.
+//   complex: A' rows 2m, 2m+1 from 4 complex k of one row m of A; B' from
+//            2 x 4 complex k of one column n of B;
+//   real:    2 x 8 k of one row of A and of one column of B.
+template <bool CPLX> struct GtRegs;
+template <> struct GtRegs<true> {
+  float2 a[4], b[8];
+};
+template <> struct GtRegs<false> {
+  float a[16], b[16];
+};
+
+// A converter thread's row of A and column of B in the current tile (null
+// when outside the problem), K and the K strides, fixed for the tile's stages.
+struct GtRows {
+  const float* a;
+  const float* b;
+  int64_t K, ask, bsk;
+  int akv, bkv;
+};
+
+template <bool CPLX>
+__device__ __forceinline__ GtRows gt_rows(const GtTile* ti, int tid) {
+  const GroupProblem& p = ti->p;
+  constexpr int E = CPLX ? 2 : 1;   // floats per element
+  const int64_t li = ti->li;
+  const int64_t m = CPLX ? ti->mt * 64 + (tid & 63) : ti->mt * 128 + (tid & 127);
+  const int64_t n = ti->nt * 128 + (tid & 127);
+  GtRows w;
+  w.a = m < p.m ? static_cast<const float*>(p.a) + E * (li * p.a_sl + m * p.a_sm) : nullptr;
+  w.b = n < p.n ? static_cast<const float*>(p.b) + E * (li * p.b_sl + n * p.b_sn) : nullptr;
+  w.K = p.k;
+  w.ask = p.a_sk;
+  w.bsk = p.b_sk;
+  w.akv = p.a_kvec;
+  w.bkv = p.b_kvec;
+  return w;
+}
+
+// 4 complex (or 8 real) consecutive k of one operand row starting at k0:
+// two 16-byte loads when the row is K-contiguous and 16-byte aligned (kvec)
+// and the run lies inside K, element loads otherwise; zeros for a null row.
+__device__ __forceinline__ void gt_ld4c(const float* rowf, int64_t sk, int64_t k0, int64_t K, int kvec,
+                                        float2* out) {
+  const float2* row = reinterpret_cast<const float2*>(rowf);
+  if (!row) {
+#pragma unroll
+    for (int j = 0; j < 4; ++j) out[j] = make_float2(0.f, 0.f);
+  } else if (kvec && k0 + 4 <= K) {
+    const float4* q = reinterpret_cast<const float4*>(row + k0);
+    const float4 u0 = __ldg(q), u1 = __ldg(q + 1);
+    out[0] = make_float2(u0.x, u0.y);
+    out[1] = make_float2(u0.z, u0.w);
+    out[2] = make_float2(u1.x, u1.y);
+    out[3] = make_float2(u1.z, u1.w);
+  } else {
+#pragma unroll
+    for (int j = 0; j < 4; ++j) out[j] = k0 + j < K ? __ldg(row + (k0 + j) * sk) : make_float2(0.f, 0.f);
+  }
+}
+__device__ __forceinline__ void gt_ld8r(const float* row, int64_t sk, int64_t k0, int64_t K, int kvec, float* out) {
+  if (!row) {
+#pragma unroll
+    for (int j = 0; j < 8; ++j) out[j] = 0.f;
+  } else if (kvec && k0 + 8 <= K) {
+    const float4* q = reinterpret_cast<const float4*>(row + k0);
+    const float4 u0 = __ldg(q), u1 = __ldg(q + 1);
+    out[0] = u0.x; out[1] = u0.y; out[2] = u0.z; out[3] = u0.w;
+    out[4] = u1.x; out[5] = u1.y; out[6] = u1.z; out[7] = u1.w;
+  } else {
+#pragma unroll
+    for (int j = 0; j < 8; ++j) out[j] = k0 + j < K ? __ldg(row + (k0 + j) * sk) : 0.f;
+  }
+}
+
+__device__ __forceinline__ void gt_load(const GtRows& w, int kt, int tid, GtRegs<true>& r) {
+  gt_ld4c(w.a, w.ask, (int64_t)kt * 16 + 4 * (tid >> 6), w.K, w.akv, r.a);
+#pragma unroll
+  for (int u = 0; u < 2; ++u) gt_ld4c(w.b, w.bsk, (int64_t)kt * 16 + 4 * ((tid >> 7) + 2 * u), w.K, w.bkv, r.b + 4 * u);
+}
+
+__device__ __forceinline__ void gt_load(const GtRows& w, int kt, int tid, GtRegs<false>& r) {
+#pragma unroll
+  for (int u = 0; u < 2; ++u) {
+    const int64_t k0 = (int64_t)kt * 32 + 8 * ((tid >> 7) + 2 * u);
+    gt_ld8r(w.a, w.ask, k0, w.K, w.akv, r.a + 8 * u);
+    gt_ld8r(w.b, w.bsk, k0, w.K, w.bkv, r.b + 8 * u);
+  }
+}
+
+// The NT BF16 terms of x (each in the upper 16 bits of t[u]; low bits are
+// rounding residue), by the integer rounding of split8_store.  The split is
+// odd in x: the terms of -x are those of x with the sign bit flipped.
+template <int NT>
+__device__ __forceinline__ void split_terms(float x, uint32_t (&t)[NT]) {
+#pragma unroll
+  for (int u = 0; u < NT; ++u) {
+    const uint32_t r = __float_as_uint(x) + 0x8000u;
+    t[u] = r;
+    if (u + 1 < NT) x -= __uint_as_float(r & 0xffff0000u);
+  }
+}
+__device__ __forceinline__ uint32_t pack_hi(uint32_t lo, uint32_t hi) { return __byte_perm(lo, hi, 0x7632); }
+
+// Split one stage's registers into NT BF16 terms in the K-major core-matrix
+// layout (8 rows x 16 bytes per core matrix; 4 k-chunks per 8-row group).
+template <int NT>
+__device__ __forceinline__ void gt_store(const GtRegs<true>& r, uint32_t st, int tid, int lane) {
+  const int ml = tid & 63, c8 = tid >> 6;
+  // Rows 2m = (re, -im) and 2m+1 = (im, re) of the embedding.  The thread
+  // stores row 2m + firstp first (each quarter-warp's 16-byte stores then hit
+  // eight distinct bank groups) as pairs (x, y); the other row's pairs are
+  // (s y, -s x) with s = +1 for firstp = 1 and -1 for firstp = 0, i.e. the
+  // same terms with the sign of one half flipped.
+  const int firstp = (lane >> 2) & 1;
+  const uint32_t flip = firstp ? 0x80000000u : 0x00008000u;
+  uint32_t tx[4][NT], ty[4][NT];
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    split_terms<NT>(firstp ? r.a[j].y : r.a[j].x, tx[j]);
+    split_terms<NT>(firstp ? r.a[j].x : -r.a[j].y, ty[j]);
+  }
+  const int r1 = 2 * ml + firstp, r2 = 2 * ml + (firstp ^ 1);
+  const uint32_t o1 = st + (uint32_t)(((r1 >> 3) * 4 + c8) * 128 + (r1 & 7) * 16);
+  const uint32_t o2 = st + (uint32_t)(((r2 >> 3) * 4 + c8) * 128 + (r2 & 7) * 16);
+#pragma unroll
+  for (int u = 0; u < NT; ++u) {
+    sts128(o1 + u * gt::TILE_BYTES, make_uint4(pack_hi(tx[0][u], ty[0][u]), pack_hi(tx[1][u], ty[1][u]),
+                                               pack_hi(tx[2][u], ty[2][u]), pack_hi(tx[3][u], ty[3][u])));
+    sts128(o2 + u * gt::TILE_BYTES,
+           make_uint4(pack_hi(ty[0][u], tx[0][u]) ^ flip, pack_hi(ty[1][u], tx[1][u]) ^ flip,
+                      pack_hi(ty[2][u], tx[2][u]) ^ flip, pack_hi(ty[3][u], tx[3][u]) ^ flip));
+  }
+  const int nl = tid & 127;
+#pragma unroll
+  for (int u = 0; u < 2; ++u) {
+    const int c8b = (tid >> 7) + 2 * u;
+    uint32_t tr[4][NT], tq[4][NT];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      split_terms<NT>(r.b[4 * u + j].x, tr[j]);
+      split_terms<NT>(r.b[4 * u + j].y, tq[j]);
+    }
+    const uint32_t ob = st + gt::Cfg<NT>::STAGE_BYTES / 2 + (uint32_t)(((nl >> 3) * 4 + c8b) * 128 + (nl & 7) * 16);
+#pragma unroll
+    for (int t = 0; t < NT; ++t)
+      sts128(ob + t * gt::TILE_BYTES, make_uint4(pack_hi(tr[0][t], tq[0][t]), pack_hi(tr[1][t], tq[1][t]),
+                                                 pack_hi(tr[2][t], tq[2][t]), pack_hi(tr[3][t], tq[3][t])));
+  }
+}
+
+template <int NT>
+__device__ __forceinline__ void gt_store(const GtRegs<false>& r, uint32_t st, int tid, int lane) {
+  (void)lane;
+  const int rl = tid & 127;
+#pragma unroll
+  for (int u = 0; u < 2; ++u) {
+    const int c8 = (tid >> 7) + 2 * u;
+    const uint32_t so = (uint32_t)(((rl >> 3) * 4 + c8) * 128 + (rl & 7) * 16);
+    float va[8], vb[8];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      va[j] = r.a[8 * u + j];
+      vb[j] = r.b[8 * u + j];
+    }
+    split8_store<NT>(va, st + so);
+    split8_store<NT>(vb, st + gt::Cfg<NT>::STAGE_BYTES / 2 + so);
+  }
+}
+
+// Wait for this CTA's tile j (tile index tl) in the scheduler ring and skip
+// forward over tiles without k stages (K = 0: releasing their slots).
+// 1: (j, tl, ti, nkt) is the next tile with stages; 0: none left; -1: aborted.
+template <bool CPLX>
+__device__ __forceinline__ int gt_next_tile(const GtArgs& t, unsigned char* slots, uint64_t* sched_full,
+                                            uint64_t* sched_empty, volatile int* abort_flag, int lane,
+                                            uint32_t& j, int64_t& tl, const GtTile*& ti, int& nkt) {
+  using namespace gt;
+  for (; tl < t.tiles; tl += gridDim.x, ++j) {
+    const int s = j % NSLOT;
+    if (!__all_sync(0xffffffffu, mbar_wait(&sched_full[s], (j / NSLOT) & 1, abort_flag))) return -1;
+    ti = reinterpret_cast<const GtTile*>(slots + s * SLOT_BYTES);
+    nkt = gt_stages<CPLX>(ti->p);
+    if (nkt > 0) return 1;
+    __syncwarp();
+    if (lane == 0) mbar_arrive(&sched_empty[s]);
+  }
+  return 0;
+}
+
+// Converter warps 0-7: every stage of every tile of this CTA, in order; the
+// loads of the next stage (of this tile or the next one) are issued before
+// the current stage is split and stored.
+template <int NT, bool CPLX>
+__device__ __forceinline__ void gt_converters(const GtArgs& t, uint32_t sbase, unsigned char* slots,
+                                              uint64_t* sched_full, uint64_t* sched_empty, uint64_t* full,
+                                              uint64_t* empty, volatile int* abort_flag, int warp, int lane) {
+  using namespace gt;
+  constexpr int STAGES = Cfg<NT>::STAGES, STAGE_BYTES = Cfg<NT>::STAGE_BYTES;
+  const int tid = warp * 32 + lane;
+  uint32_t j = 0;
+  int64_t tile = blockIdx.x;
+  const GtTile* cur = nullptr;
+  int nk = 0;
+  if (gt_next_tile<CPLX>(t, slots, sched_full, sched_empty, abort_flag, lane, j, tile, cur, nk) <= 0) return;
+  GtRegs<CPLX> r0, r1;
+  GtRows w = gt_rows<CPLX>(cur, tid);
+  gt_load(w, 0, tid, r0);
+  int kt = 0;
+  uint32_t it = 0;
+  while (true) {
+    uint32_t jn = j;
+    int64_t tn = tile;
+    const GtTile* nx = cur;
+    int nkn = nk, kn = kt + 1;
+    bool more = true;
+    if (kn == nk) {   // this is the tile's last stage: the next one is the next tile's first
+      jn = j + 1;
+      tn = tile + gridDim.x;
+      kn = 0;
+      const int rn = gt_next_tile<CPLX>(t, slots, sched_full, sched_empty, abort_flag, lane, jn, tn, nx, nkn);
+      if (rn < 0) return;
+      more = rn == 1;
+    }
+    if (more) {
+      if (kn == 0) w = gt_rows<CPLX>(nx, tid);   // the next tile's rows (this tile's loads are all issued)
+      gt_load(w, kn, tid, r1);
+    }
+    const int s = it % STAGES;
+    if (it >= (uint32_t)STAGES &&
+        !__all_sync(0xffffffffu, mbar_wait(&empty[s], ((it / STAGES) - 1) & 1, abort_flag)))
+      return;
+    gt_store<NT>(r0, sbase + s * STAGE_BYTES, tid, lane);
+    fence_proxy_async();
+    __syncwarp();
+    if (lane == 0) mbar_arrive(&full[s]);
+    ++it;
+    if (kn == 0 && lane == 0) mbar_arrive(&sched_empty[j % NSLOT]);   // done with tile j's slot
+    if (!more) return;
+    j = jn;
+    tile = tn;
+    cur = nx;
+    nk = nkn;
+    kt = kn;
+    r0 = r1;
+  }
+}
+
+// Write 16 columns (colbase .. +15 of the tile) of accumulator row `row`
+// through the alpha-beta epilogue.  Complex: the row is real row 2m + part of
+// the embedding; the element's other part is in the neighbouring lane, and
+// each lane reads and writes only its own part.
+template <bool CPLX>
+__device__ __forceinline__ void gt_store_cols(const GtArgs& t, const GtTile* ti, int row, int colbase,
+                                              const float (&v)[16]) {
+  const GroupProblem& p = ti->p;
+  const int64_t pm = p.m, pn = p.n, csm = p.c_sm, csn = p.c_sn, n0 = ti->nt * 128 + colbase;
+  if constexpr (CPLX) {
+    const cf32 sx = scalar_as<cf32>(t.sx), sy = scalar_as<cf32>(t.sy);
+    const int part = row & 1;
+    const int64_t m = ti->mt * 64 + (row >> 1);
+    float* C = static_cast<float*>(p.c) + 2 * (ti->li * p.c_sl + m * csm) + part;
+    const bool mrow = m < pm;
+    if (t.sy_zero && sx.im == 0.f) {   // a real scale of each part: no exchange between the lanes
+      if (!mrow) return;
+      const int64_t nv = pn - n0;
+      float* cp = C + 2 * n0 * csn;
+#pragma unroll
+      for (int j = 0; j < 16; ++j, cp += 2 * csn)
+        if (j < nv) *cp = sx.re * v[j];
+      return;
+    }
+#pragma unroll
+    for (int j = 0; j < 16; ++j) {
+      const int64_t n = n0 + j;
+      const bool in = mrow && n < pn;   // the same for both lanes of an element
+      float* cp = C + 2 * n * csn;
+      const float y = in && !t.sy_zero ? *cp : 0.f;
+      const float w = __shfl_xor_sync(0xffffffffu, v[j], 1), yo = __shfl_xor_sync(0xffffffffu, y, 1);
+      if (in) {
+        const float fr = part ? w : v[j], fi = part ? v[j] : w;
+        const float yr = part ? yo : y, yi = part ? y : yo;
+        float orr = t.sx_one ? fr : sx.re * fr - sx.im * fi;
+        float oi = t.sx_one ? fi : sx.re * fi + sx.im * fr;
+        if (!t.sy_zero) {
+          orr += sy.re * yr - sy.im * yi;
+          oi += sy.re * yi + sy.im * yr;
+        }
+        *cp = part ? oi : orr;
+      }
+    }
+  } else {
+    const float sx = scalar_as<float>(t.sx), sy = scalar_as<float>(t.sy);
+    const int64_t m = ti->mt * 128 + row;
+    if (m >= pm) return;
+    const int64_t nv = pn - n0;
+    float* cp = static_cast<float*>(p.c) + ti->li * p.c_sl + m * csm + n0 * csn;
+    if (t.sy_zero) {
+#pragma unroll
+      for (int j = 0; j < 16; ++j, cp += csn)
+        if (j < nv) *cp = sx * v[j];
+    } else {
+#pragma unroll
+      for (int j = 0; j < 16; ++j, cp += csn)
+        if (j < nv) *cp = fmaf(sy, *cp, sx * v[j]);
+    }
+  }
+}
+
+// Drain warps 8-11 (dw = warp - 8): thread = accumulator row 32 dw + lane
+// (the TMEM lanes of its warp quarter), all 128 columns.
+// Chunks before a tile's last go into the running sums; the last chunk is
+// added to them and written out straight from TMEM.
+template <int NT, bool CPLX>
+__device__ __forceinline__ void gt_drain(const GtArgs& t, float* acc, uint32_t tmem, unsigned char* slots,
+                                         uint64_t* sched_full, uint64_t* sched_empty, uint64_t* chunk_done,
+                                         uint64_t* drained, volatile int* abort_flag, int dw, int lane) {
+  using namespace gt;
+  const int row = 32 * dw + lane;
+  const uint32_t lane_off = (uint32_t)(32 * dw) << 16;
+  uint32_t gc = 0, j = 0;
+  for (int64_t tile = blockIdx.x; tile < t.tiles; tile += gridDim.x, ++j) {
+    const int ss = j % NSLOT;
+    if (!__all_sync(0xffffffffu, mbar_wait(&sched_full[ss], (j / NSLOT) & 1, abort_flag))) return;
+    const GtTile* ti = reinterpret_cast<const GtTile*>(slots + ss * SLOT_BYTES);
+    const int nch = (gt_stages<CPLX>(ti->p) + CHUNK - 1) / CHUNK;
+    for (int ci = 0; ci < nch; ++ci, ++gc) {
+      const int b = gc & 1;
+      if (!__all_sync(0xffffffffu, mbar_wait(&chunk_done[b], (gc >> 1) & 1, abort_flag))) return;
+      tc_fence_after();
+      const bool last = ci + 1 == nch;
+#pragma unroll 1
+      for (int hh = 0; hh < 8; ++hh) {
+        uint32_t rm[16], rc[16];
+        const uint32_t col = (uint32_t)(16 * hh);
+        tmem_ld16_nw(tmem + (uint32_t)(256 * b) + lane_off + col, rm);
+        tmem_ld16_nw(tmem + (uint32_t)(256 * b + 128) + lane_off + col, rc);
+        tmem_wait_ld();
+        float v[16];
+#pragma unroll
+        for (int jj = 0; jj < 16; ++jj) {
+          v[jj] = __uint_as_float(rm[jj]) + __uint_as_float(rc[jj]);
+          float* a = acc + (col + jj) * BM + row;
+          if (ci > 0) v[jj] += *a;
+          if (!last) *a = v[jj];
+        }
+        if (last) gt_store_cols<CPLX>(t, ti, row, (int)col, v);
+      }
+      tc_fence_before();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&drained[b]);
+    }
+    if (nch == 0) {   // K = 0: the product is zero
+      float v[16];
+#pragma unroll
+      for (int jj = 0; jj < 16; ++jj) v[jj] = 0.f;
+#pragma unroll 1
+      for (int hh = 0; hh < 8; ++hh) gt_store_cols<CPLX>(t, ti, row, 16 * hh, v);
+    }
+    __syncwarp();
+    if (lane == 0) mbar_arrive(&sched_empty[ss]);
+  }
+}
+
+template <int NT, bool CPLX>
+__global__ void __launch_bounds__(gt::NTHREADS, 1) k_group_tc(const __grid_constant__ GtArgs t) {
+  using namespace gt;
+  constexpr int STAGES = Cfg<NT>::STAGES, STAGE_BYTES = Cfg<NT>::STAGE_BYTES;
+  extern __shared__ __align__(128) unsigned char gt_raw[];
+  const uint32_t raw = smem_u32(gt_raw);
+  const uint32_t pad = (128u - (raw & 127u)) & 127u;
+  unsigned char* smem = gt_raw + pad;
+  const uint32_t sbase = raw + pad;
+  float* acc = reinterpret_cast<float*>(smem + STAGES * STAGE_BYTES);   // [BN][BM] running sums
+  unsigned char* slots = smem + STAGES * STAGE_BYTES + ACC_BYTES;       // scheduler ring
+  uint64_t* full = reinterpret_cast<uint64_t*>(slots + NSLOT * SLOT_BYTES);
+  uint64_t* empty = full + STAGES;
+  uint64_t* chunk_done = empty + STAGES;   // [2]
+  uint64_t* drained = chunk_done + 2;      // [2]
+  uint64_t* final_bar = drained + 2;
+  uint64_t* sched_full = final_bar + 1;    // [NSLOT]
+  uint64_t* sched_empty = sched_full + NSLOT;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(sched_empty + NSLOT);
+  volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  if (tid == 0) {
+    for (int s = 0; s < STAGES; ++s) {
+      mbar_init(&full[s], 8);
+      mbar_init(&empty[s], 1);
+    }
+    for (int b = 0; b < 2; ++b) {
+      mbar_init(&chunk_done[b], 1);
+      mbar_init(&drained[b], 4);
+    }
+    mbar_init(final_bar, 1);
+    for (int s = 0; s < NSLOT; ++s) {
+      mbar_init(&sched_full[s], 1);
+      mbar_init(&sched_empty[s], SLOT_USERS);
+    }
+    *abort_flag = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 12) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                 "r"(TMEM_COLS)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tmem_slot;
+
+  if (warp < 8) {
+    gt_converters<NT, CPLX>(t, sbase, slots, sched_full, sched_empty, full, empty, abort_flag, warp, lane);
+  } else if (warp < 12) {
+    gt_drain<NT, CPLX>(t, acc, tmem, slots, sched_full, sched_empty, chunk_done, drained, abort_flag, warp - 8,
+                       lane);
+  } else if (warp == 13) {
+    gt_scheduler(t, slots, sched_full, sched_empty, abort_flag, lane);
+  } else if (lane == 0) {
+    // ---------------- MMA issue ----------------
+    uint32_t it = 0, gc = 0, j = 0;
+    bool ok = true;
+    for (int64_t tile = blockIdx.x; tile < t.tiles && ok; tile += gridDim.x, ++j) {
+      const int ss = j % NSLOT;
+      if (!mbar_wait(&sched_full[ss], (j / NSLOT) & 1, abort_flag)) break;
+      const int nkt = gt_stages<CPLX>(reinterpret_cast<const GtTile*>(slots + ss * SLOT_BYTES)->p);
+      mbar_arrive(&sched_empty[ss]);
+      for (int kt = 0; kt < nkt; ++kt, ++it) {
+        const uint32_t c = gc + kt / CHUNK;
+        const int b = c & 1;
+        const bool first = kt % CHUNK == 0;
+        if (first && c >= 2 && !mbar_wait(&drained[b], ((c >> 1) - 1) & 1, abort_flag)) { ok = false; break; }
+        const int s = it % STAGES;
+        if (!mbar_wait(&full[s], (it / STAGES) & 1, abort_flag)) { ok = false; break; }
+        tc_fence_after();
+        const uint32_t sb = sbase + s * STAGE_BYTES;
+#pragma unroll
+        for (int kk = 0; kk < 2; ++kk) {
+          const uint32_t off = kk * 256;
+          uint64_t ad[NT], bdsc[NT];
+#pragma unroll
+          for (int u = 0; u < NT; ++u) {
+            ad[u] = umma_desc(sb + u * TILE_BYTES + off);
+            bdsc[u] = umma_desc(sb + (NT + u) * TILE_BYTES + off);
+          }
+          const uint32_t keep = (first && kk == 0) ? 0u : 1u;
+          umma_bf16(tmem + (uint32_t)(256 * b), ad[0], bdsc[0], keep);
+          bool first_cross = true;
+#pragma unroll
+          for (int d = 1; d < NT; ++d)
+#pragma unroll
+            for (int i = 0; i <= d; ++i) {
+              umma_bf16(tmem + (uint32_t)(256 * b + 128), ad[i], bdsc[d - i], first_cross ? keep : 1u);
+              first_cross = false;
+            }
+        }
+        umma_commit(&empty[s]);
+        if (kt % CHUNK == CHUNK - 1 || kt == nkt - 1) umma_commit(&chunk_done[b]);
+      }
+      gc += (uint32_t)((nkt + CHUNK - 1) / CHUNK);
+    }
+    umma_commit(final_bar);
+    mbar_wait_quiesce(final_bar, 0);
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 12) {
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(gt::TMEM_COLS) : "memory");
+  }
+}
+
+namespace {
+template <int NT, bool CPLX>
+cudaError_t launch_gt(const GtArgs& t, int grid, cudaStream_t s) {
+  static bool attr = false;
+  if (!attr) {
+    cudaError_t e = cudaFuncSetAttribute(k_group_tc<NT, CPLX>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         gt::Cfg<NT>::SMEM_BYTES);
+    if (e != cudaSuccess) return e;
+    attr = true;
+  }
+  k_group_tc<NT, CPLX><<<grid, gt::NTHREADS, gt::Cfg<NT>::SMEM_BYTES, s>>>(t);
+  return cudaGetLastError();
+}
+}  // namespace
+
+cudaError_t launch_group_tc(ome_dtype dt, int nterms, const GroupProblem* probs, const int32_t* tile_prob, int nprob,
+                            int64_t tiles, int grid, const Scalar& sx, const Scalar& sy, int sy_zero, int sx_one,
+                            cudaStream_t s) {
+  if ((dt != OME_F32 && dt != OME_C32) || (nterms != 2 && nterms != 3) || !tile_prob) return cudaErrorNotSupported;
+  if (tiles == 0) return cudaSuccess;
+  GtArgs t;
+  memset(&t, 0, sizeof(t));
+  t.probs = probs;
+  t.tile_prob = tile_prob;
+  t.nprob = nprob;
+  t.tiles = tiles;
+  t.sx = sx;
+  t.sy = sy;
+  t.sy_zero = sy_zero;
+  t.sx_one = sx_one;
+  cudaError_t e;
+  {
+    KernelTimer kt(s, "k_group_tc");
+    if (dt == OME_C32) e = nterms == 3 ? launch_gt<3, true>(t, grid, s) : launch_gt<2, true>(t, grid, s);
+    else e = nterms == 3 ? launch_gt<3, false>(t, grid, s) : launch_gt<2, false>(t, grid, s);
+  }
+  count_launch();
+  return e;
+}
+
 // One thread waits on an mbarrier that nothing arrives on, bounded by
 // wait_ns; on expiry it records the timeout like any stalled wait and exits.
 __global__ void k_selftest_wait(uint64_t wait_ns) {

@@ -114,6 +114,31 @@ cudaError_t launch_gemm_tma2(const GemmArgs& g, int nterms, void* workspace, siz
 
 // Read and clear the CUDA-core GEMM's split-partial self-check flag.
 int simt_bounds_flag();
+// One problem of a grouped launch: C[m,n,l] = sx * sum_k A[m,k,l] B[k,n,l]
+// (+ sy*C), strides in elements; tile_begin / tiles_m / tiles_n depend on
+// the tile shape of the kernel the table is built for.
+struct GroupProblem {
+  const void* a;
+  const void* b;
+  void* c;
+  int64_t m, n, k, l;
+  int64_t a_sm, a_sk, a_sl;
+  int64_t b_sk, b_sn, b_sl;
+  int64_t c_sm, c_sn, c_sl;
+  int64_t tile_begin;  // first global tile index of this problem
+  int32_t tiles_m, tiles_n;
+  // the operand's K mode is contiguous and its rows start on 16 bytes
+  // (vector loads of 4 complex / 8 real k by the tensor-core kernel)
+  int32_t a_kvec, b_kvec;
+};
+// Grouped launch on the tensor cores (F32, or C32 through its real 2 x 2
+// embedding): 128 x 128 tiles of the (embedded) output, BF16 split products
+// (nterms 2 or 3) formed in shared memory; tiles_m counts 128 real rows
+// (64 complex rows for C32).  cudaErrorNotSupported for other dtypes.
+// tile_prob[t] is the problem that owns global tile t.
+cudaError_t launch_group_tc(ome_dtype dt, int nterms, const GroupProblem* probs, const int32_t* tile_prob, int nprob,
+                            int64_t tiles, int grid, const Scalar& sx, const Scalar& sy, int sy_zero, int sx_one,
+                            cudaStream_t s);
 // Synchronise s and read/clear the device timeout flag: 1 if a bounded wait
 // gave up, 0 if not, -cudaError on failure.
 int device_status(cudaStream_t s);

@@ -1,6 +1,9 @@
 """Batched contractions of uneven shapes (one grouped launch) against the
 oracle: MPS transfer contractions (ab,bcd)->acd, (acd,de)->ace in ComplexF32
-with random bond dimensions, plus exact Int64 and tropical batches."""
+with random bond dimensions, plus exact Int64 and tropical batches.  Tile
+config 3 is the tensor-core grouped kernel (BF16x6 split products; ComplexF32
+through its real 2 x 2 embedding), held to the same 1e-5 as the CUDA-core
+tiles."""
 import numpy as np
 import pytest
 import torch
@@ -22,7 +25,7 @@ def mps_jobs(n, seed):
     return jobs
 
 
-@pytest.mark.parametrize("tile_config", [-1, 0, 2])
+@pytest.mark.parametrize("tile_config", [-1, 0, 2, 3])
 def test_mps_transfer_batch_complex64(tile_config):
     rng = np.random.default_rng(9)
     jobs = mps_jobs(40, 9)
@@ -68,3 +71,45 @@ def test_batch_rejects_unmergeable_groups():
     with pytest.raises(ome.OMEError):
         # output (k, i, j) of x1's (i, j): i and j are not adjacent in the output -> two M modes
         ome.BatchedEinsum(ome.ein("ijl,lk->ikj"), [(x, torch.zeros(4, 4, device="cuda"))])
+
+
+def _tc_kernel_ran(fn):
+    from test_gpu_parity import kernel_names
+    _, names = kernel_names(fn)
+    return "k_group_tc" in names
+
+
+@pytest.mark.parametrize("dt", ["f32", "c64"])
+def test_tensor_core_group_uneven_alpha_beta(dt):
+    """Uneven problems (ragged M, N, K around the 128 x 128 x 32 tiles, K = 1,
+    a batch mode, transposed operands) with y = 2.5 x1 x2 - 0.75 y (complex:
+    (1.5 - 0.5i) x1 x2 + (0.25 + 1i) y)."""
+    rng = np.random.default_rng(21)
+    shapes = [(1, 1, 1, 1), (127, 33, 129, 1), (128, 32, 128, 1), (129, 31, 257, 2), (300, 1, 64, 1),
+              (17, 513, 200, 3), (64, 64, 64, 5), (250, 100, 3, 1), (2, 700, 2, 1)]
+    cplx = dt == "c64"
+    sx = complex(1.5, -0.5) if cplx else 2.5
+    sy = complex(0.25, 1.0) if cplx else -0.75
+    xs_list, ys, wants = [], [], []
+    for (m, k, n, l) in shapes:
+        a, b = gen(rng, (k, m, l), dt), gen(rng, (k, n, l), dt)   # x1 K-major (k first)
+        y0 = gen(rng, (m, n, l), dt)
+        xs_list.append((to_dev(a, dt), to_dev(b, dt)))
+        ys.append(to_dev(y0, dt))
+        wide = np.complex128 if cplx else np.float64
+        ab = O.einsum([("k", "i", "l"), ("k", "j", "l")], ("i", "j", "l"), [a.astype(wide), b.astype(wide)],
+                      {"i": m, "j": n, "k": k, "l": l})
+        wants.append(sx * ab + sy * y0.astype(ab.dtype))
+    bt = ome.BatchedEinsum(ome.ein("kil,kjl->ijl"), xs_list, ys=ys, tile_config=3)
+    assert bt.tile_config == 3
+    assert _tc_kernel_ran(lambda: bt.run(sx, sy))
+    for y, w in zip(bt.outputs, wants):
+        assert relerr(to_np(y), w) < 1e-5
+
+
+def test_tensor_core_group_rejects_other_dtypes():
+    x = torch.zeros(8, 8, dtype=torch.int64, device="cuda")
+    with pytest.raises(ome.OMEError):
+        ome.BatchedEinsum(ome.ein("ij,jk->ik"), [(x, x)], tile_config=3)
+    bt = ome.BatchedEinsum(ome.ein("ij,jk->ik"), [(x, x)])   # autotune skips the tensor-core kernel
+    assert bt.tuned_us[3] == -1 and bt.tile_config != 3
