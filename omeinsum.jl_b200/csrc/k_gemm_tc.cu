@@ -2413,61 +2413,84 @@ __device__ __forceinline__ int gt_next_tile(const GtArgs& t, unsigned char* slot
   return 0;
 }
 
-// Converter warps 0-7: every stage of every tile of this CTA, in order; the
-// loads of the next stage (of this tile or the next one) are issued before
-// the current stage is split and stored.
+// Converter warps 0-7: every stage of every tile of this CTA, in order.  A
+// load cursor runs PD stages (of this tile or the following ones) ahead of
+// the stage being split and stored, so PD stages of global loads are in
+// flight while a thread converts.
+template <bool CPLX>
+struct GtCursor {
+  uint32_t j;            // position of the cursor's tile in this CTA's sequence
+  int64_t tile;
+  const GtTile* ti;
+  int nk, kt;
+  bool more;
+  GtRows w;
+};
+
+// Issue the loads of the cursor's stage into r, note whether it ends its tile
+// (rel = the tile's slot, else -1) and step the cursor.  False when aborted.
+template <bool CPLX>
+__device__ __forceinline__ bool gt_issue(const GtArgs& t, unsigned char* slots, uint64_t* sched_full,
+                                         uint64_t* sched_empty, volatile int* abort_flag, int tid, int lane,
+                                         GtCursor<CPLX>& c, GtRegs<CPLX>& r, int& rel, bool& have) {
+  have = c.more;
+  if (!c.more) return true;
+  gt_load(c.w, c.kt, tid, r);
+  rel = c.kt + 1 == c.nk ? (int)(c.j % gt::NSLOT) : -1;
+  if (++c.kt == c.nk) {
+    ++c.j;
+    c.tile += gridDim.x;
+    c.kt = 0;
+    const int rn = gt_next_tile<CPLX>(t, slots, sched_full, sched_empty, abort_flag, lane, c.j, c.tile, c.ti, c.nk);
+    if (rn < 0) return false;
+    c.more = rn == 1;
+    if (c.more) c.w = gt_rows<CPLX>(c.ti, tid);
+  }
+  return true;
+}
+
 template <int NT, bool CPLX>
 __device__ __forceinline__ void gt_converters(const GtArgs& t, uint32_t sbase, unsigned char* slots,
                                               uint64_t* sched_full, uint64_t* sched_empty, uint64_t* full,
                                               uint64_t* empty, volatile int* abort_flag, int warp, int lane) {
   using namespace gt;
   constexpr int STAGES = Cfg<NT>::STAGES, STAGE_BYTES = Cfg<NT>::STAGE_BYTES;
+  constexpr int PD = CPLX ? 2 : 1;   // register budget: 24 floats a stage (complex), 32 (real)
   const int tid = warp * 32 + lane;
-  uint32_t j = 0;
-  int64_t tile = blockIdx.x;
-  const GtTile* cur = nullptr;
-  int nk = 0;
-  if (gt_next_tile<CPLX>(t, slots, sched_full, sched_empty, abort_flag, lane, j, tile, cur, nk) <= 0) return;
-  GtRegs<CPLX> r0, r1;
-  GtRows w = gt_rows<CPLX>(cur, tid);
-  gt_load(w, 0, tid, r0);
-  int kt = 0;
+  GtCursor<CPLX> c;
+  c.j = 0;
+  c.tile = blockIdx.x;
+  c.kt = 0;
+  const int rc = gt_next_tile<CPLX>(t, slots, sched_full, sched_empty, abort_flag, lane, c.j, c.tile, c.ti, c.nk);
+  if (rc <= 0) return;
+  c.more = true;
+  c.w = gt_rows<CPLX>(c.ti, tid);
+  GtRegs<CPLX> r[PD + 1];
+  int rel[PD + 1];
+  bool have[PD + 1];
+#pragma unroll
+  for (int q = 0; q < PD; ++q)
+    if (!gt_issue<CPLX>(t, slots, sched_full, sched_empty, abort_flag, tid, lane, c, r[q], rel[q], have[q])) return;
   uint32_t it = 0;
-  while (true) {
-    uint32_t jn = j;
-    int64_t tn = tile;
-    const GtTile* nx = cur;
-    int nkn = nk, kn = kt + 1;
-    bool more = true;
-    if (kn == nk) {   // this is the tile's last stage: the next one is the next tile's first
-      jn = j + 1;
-      tn = tile + gridDim.x;
-      kn = 0;
-      const int rn = gt_next_tile<CPLX>(t, slots, sched_full, sched_empty, abort_flag, lane, jn, tn, nx, nkn);
-      if (rn < 0) return;
-      more = rn == 1;
-    }
-    if (more) {
-      if (kn == 0) w = gt_rows<CPLX>(nx, tid);   // the next tile's rows (this tile's loads are all issued)
-      gt_load(w, kn, tid, r1);
-    }
+  while (have[0]) {
+    if (!gt_issue<CPLX>(t, slots, sched_full, sched_empty, abort_flag, tid, lane, c, r[PD], rel[PD], have[PD]))
+      return;
     const int s = it % STAGES;
     if (it >= (uint32_t)STAGES &&
         !__all_sync(0xffffffffu, mbar_wait(&empty[s], ((it / STAGES) - 1) & 1, abort_flag)))
       return;
-    gt_store<NT>(r0, sbase + s * STAGE_BYTES, tid, lane);
+    gt_store<NT>(r[0], sbase + s * STAGE_BYTES, tid, lane);
     fence_proxy_async();
     __syncwarp();
     if (lane == 0) mbar_arrive(&full[s]);
     ++it;
-    if (kn == 0 && lane == 0) mbar_arrive(&sched_empty[j % NSLOT]);   // done with tile j's slot
-    if (!more) return;
-    j = jn;
-    tile = tn;
-    cur = nx;
-    nk = nkn;
-    kt = kn;
-    r0 = r1;
+    if (rel[0] >= 0 && lane == 0) mbar_arrive(&sched_empty[rel[0]]);   // done with that tile's slot
+#pragma unroll
+    for (int q = 0; q < PD; ++q) {
+      r[q] = r[q + 1];
+      rel[q] = rel[q + 1];
+      have[q] = have[q + 1];
+    }
   }
 }
 
