@@ -167,8 +167,9 @@ def cpu_suite(O, inputs, steps=1, results=None):
 
 
 def relerr(got, want):
-    got = np.asarray(got, dtype=np.float64)
-    want = np.asarray(want, dtype=np.float64)
+    wide = np.complex128 if np.iscomplexobj(got) or np.iscomplexobj(want) else np.float64
+    got = np.asarray(got, dtype=wide)
+    want = np.asarray(want, dtype=wide)
     n = max(np.linalg.norm(got.ravel()), np.linalg.norm(want.ravel()))
     d = np.linalg.norm((got - want).ravel())
     return 0.0 if d == 0 else float(d / max(n, 1e-300))
@@ -330,6 +331,17 @@ def tn_section(ome, dev, n=180, sc_target=27):
     for k in ("fp32", "bf16x6", "bf16x3"):
         out[k]["rel_err_vs_fp64"] = abs(vals[k] - vals["fp64"]) / abs(vals["fp64"])
         out[k]["contractions_per_s"] = 1.0 / out[k]["s"]
+    for k in ("fp64", "fp32", "bf16x6", "bf16x3"):
+        out[k]["tflops"] = out["flops_per_contraction"] / out[k]["s"] / 1e12
+    # each arm against its own peak: plain FP32 against the CUDA cores' FP32
+    # FMA rate (148 SMs x 128 lanes x 2 flops at the 1965 MHz maximum clock),
+    # the split products against measured bf16 / (number of BF16 MMAs)
+    _, bf16, src = load_peaks()
+    fp32_peak = 148 * 128 * 2 * 1.965e9 / 1e12
+    out["fp32"]["frac_of_fp32_cuda_core_peak"] = out["fp32"]["tflops"] / fp32_peak
+    out["fp32"]["peak"] = {"tflops": fp32_peak, "source": "nominal: 148 SMs x 128 FP32 lanes x 2 x 1965 MHz"}
+    out["bf16x6"]["frac_of_bf16x6_peak"] = out["bf16x6"]["tflops"] / (bf16 / 6)
+    out["bf16x3"]["frac_of_bf16x3_peak"] = out["bf16x3"]["tflops"] / (bf16 / 3)
     out["speedup_bf16x6_vs_fp32"] = out["fp32"]["s"] / out["bf16x6"]["s"]
     ome.set_einsum_backend(ome.B200Backend())
     return out
@@ -427,7 +439,8 @@ def batch_section(ome, dev, njobs=8192, seed=9):
     for j, x in zip(sd[:nref], X[:nref]):
         m = ome.einsum(code1, [x[0].to(torch.complex128), x[1].to(torch.complex128)], j)
         refs.append(ome.einsum(code2, [m, x[2].to(torch.complex128)], j))
-    forced = {}
+    forced, sampled = {}, {}
+    nsmp = 32   # jobs whose results the CPU leg checks against the oracle
     for cfg in (1, 3):
         f1 = ome.BatchedEinsum(code1, [(x[0], x[1]) for x in X], tile_config=cfg)
         f2 = ome.BatchedEinsum(code2, [(t, x[2]) for t, x in zip(f1.outputs, X)], tile_config=cfg)
@@ -437,6 +450,7 @@ def batch_section(ome, dev, njobs=8192, seed=9):
              for y, r in zip(f2.outputs[:nref], refs)]
         forced[cfg] = {"graph_ms": ms, "tflops": flops / (ms / 1e3) / 1e12,
                        "rel_err_vs_c128": {"jobs": nref, "max": max(e), "median": float(np.median(e))}}
+        sampled[cfg] = [y.cpu().numpy() for y in f2.outputs[:nsmp]]
         del fg, f1, f2
     _, bf16, src = load_peaks()
     tc_peak = bf16 / 6   # 4 real products x 6 BF16 MMAs = 48 BF16 flops per complex multiply-add (8 flops)
@@ -454,7 +468,9 @@ def batch_section(ome, dev, njobs=8192, seed=9):
             "tile_config": [b1.tile_config, b2.tile_config], "autotune_us": [b1.tuned_us, b2.tuned_us],
             "tile_configs": "0-2 CUDA-core 32x32, 64x32, 64x64 tiles; 3 tensor cores (k_group_tc)",
             "cuda_core_cfg1": forced[1], "tensor_core_cfg3": forced[3],
-            "max_rel_diff_grouped_vs_loop": err}
+            "max_rel_diff_grouped_vs_loop": err,
+            "_oracle_samples": [(j, [t.cpu().numpy() for t in x], sampled[1][i], sampled[3][i])
+                                for i, (j, x) in enumerate(zip(sd[:nsmp], X[:nsmp]))]}
 
 
 def serve_section(ome, dev, njobs=400, rate=2000.0, seed=10, nmin=40, nmax=200, grad_frac=0.1, cap_s=120.0,
@@ -781,6 +797,19 @@ def main():
     torch.cuda.empty_cache()
     sharded = tn_sharded_section(ome, dev, world) if (grouped and not args.no_tn) else None
     batch = None if (args.no_batch or world > 1) else batch_section(ome, dev)
+    if batch is not None:
+        smp = batch.pop("_oracle_samples")
+        if cpu is not None:   # the CPU leg ran: check sampled jobs of both kernels against the oracle
+            ne = O.parse_nested("(ab,bcd),de->ace")
+            errs = {1: [], 3: []}
+            for j, xs, y1, y3 in smp:
+                want = O.nested_einsum(ne, [x.astype(np.complex128) for x in xs], j)
+                errs[1].append(relerr(y1, want))
+                errs[3].append(relerr(y3, want))
+            for cfg, key in ((1, "cuda_core_cfg1"), (3, "tensor_core_cfg3")):
+                batch[key]["rel_err_vs_oracle"] = {"jobs": len(smp), "max": max(errs[cfg]),
+                                                   "median": float(np.median(errs[cfg])),
+                                                   "reference": "oracle (ComplexF64 NumPy restatement)"}
     serve = None if (args.no_serve or world > 1) else serve_section(ome, dev)
     detail = {}
     for (nm, code, ext, _), ms in zip(CASES, per_case):
