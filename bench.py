@@ -378,6 +378,37 @@ def tn_sharded_section(ome, dev, world, n=180, sc_target=27):
             "parallelism": "contiguous slice ranges per rank, one NCCL all-reduce of the FP64 partial"}
 
 
+def run_group_case(ome, dev, njobs, seed=9):
+    """Profiling aid: the first contraction ab,bcd->acd of njobs MPS transfer
+    jobs (the batching section's distribution) as one grouped launch on the
+    tensor-core kernel (tile config 3): 3 warm-up launches, 5 timed."""
+    import torch
+    jobs = mps_jobs(njobs, seed)
+    g = torch.Generator(device=dev).manual_seed(seed)
+
+    def cx(*shape):
+        r = torch.randn(*shape[::-1], generator=g, device=dev)
+        i = torch.randn(*shape[::-1], generator=g, device=dev)
+        return torch.complex(r, i).permute(*range(len(shape) - 1, -1, -1))
+
+    X = [(cx(j["a"], j["b"]), cx(j["b"], j["c"], j["d"])) for j in jobs]
+    b1 = ome.BatchedEinsum(ome.ein("ab,bcd->acd"), X, tile_config=3)
+    for _ in range(3):
+        b1.run()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(5):
+        b1.run()
+    e1.record()
+    torch.cuda.synchronize()
+    ome.device_status()
+    flops = sum(8 * j["a"] * j["b"] * j["c"] * j["d"] for j in jobs)
+    ms = e0.elapsed_time(e1) / 5
+    print(json.dumps({"group_case": f"{njobs} x ab,bcd->acd ComplexF32, tile config 3", "ms_per_launch": ms,
+                      "complex_tflops": flops / (ms / 1e3) / 1e12}))
+
+
 def mps_jobs(njobs, seed):
     rng = np.random.default_rng(seed)
     jobs = []
@@ -594,6 +625,8 @@ def main():
                     help="run the slice-sharded network section at N=1 too (a one-rank NCCL group)")
     ap.add_argument("--case", default=None,
                     help="profiling aid: run only this suite contraction (e.g. 'ijk->j') twice and exit")
+    ap.add_argument("--group-case", type=int, default=0,
+                    help="profiling aid: one grouped tensor-core launch over this many MPS jobs (ab,bcd->acd)")
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -622,6 +655,8 @@ def main():
     lib = ome.load_library()
     if args.case is not None:
         return run_case_only(ome, args.case, dev)
+    if args.group_case:
+        return run_group_case(ome, dev, args.group_case)
 
     hosts, devs, outs, codes = [], [], [], []
     for name, code, ext, seed in CASES:

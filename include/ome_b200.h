@@ -299,6 +299,75 @@ OME_API int ome_batch_run(ome_ctx* ctx, ome_batch* batch, void* stream, const vo
 OME_API int ome_batch_info(const ome_batch* batch, int32_t* tile_config, float* tuned_us);
 OME_API int ome_batch_destroy(ome_batch* batch);
 
+/* A CUDA graph of grouped launches (e.g. the two contractions of an MPS sweep
+ * step), captured once and replayed with one call: replaces a loop of
+ * ome_batch_run calls whose host launch cost would dominate small batches.
+ * The graph runs batches[0..count) in order, each with its chosen kernel, with
+ * scalars sxs[i] / sys[i] (NULL arrays or entries: 1 and 0 of the batch's
+ * dtype).  The batches must outlive the graph; replays read the tensors bound
+ * at batch creation.  Capture uses a private stream after synchronising
+ * `stream`; ome_graph_launch enqueues one replay on `stream`. */
+typedef struct ome_graph ome_graph;
+OME_API int ome_batch_graph_create(ome_ctx* ctx, void* stream, int32_t count, ome_batch* const* batches,
+                                   const void* const* sxs, const void* const* sys, ome_graph** out);
+OME_API int ome_graph_launch(ome_graph* graph, void* stream);
+OME_API int ome_graph_destroy(ome_graph* graph);
+
+/* Serving: continuous batching of whole contraction-tree jobs --------------
+ *
+ * No counterpart in the reference, whose service would call
+ * einsum(::NestedEinsum) or cost_and_gradient (src/einsequence.jl:270-287,
+ * src/bp.jl:122-130) once per request.  A server keeps n_slots slots on one
+ * device; each owns a stream, a host issue thread and a context whose
+ * workspace is hbm_budget_bytes / n_slots (allocated on the slot's first job,
+ * kept until ome_server_destroy).  Jobs are admitted in arrival order when a
+ * slot is free and the plan's peak workspace bytes (ome_plan_peak_bytes:
+ * forward, or forward+gradient for gradient jobs) fit a slot's share; a job
+ * above a share but within the budget waits until every slot is idle and runs
+ * alone in a workspace of its own size; jobs above the budget
+ * (OME_JOB_REJECTED_MEMORY) or with more than max_job_work multiply-adds
+ * (OME_JOB_REJECTED_WORK; max_job_work <= 0: no cap) are rejected at
+ * admission.  Admission and retirement happen in ome_server_poll, which never
+ * blocks on the device. */
+typedef struct ome_server ome_server;
+typedef enum {
+  OME_JOB_COMPLETED = 0,
+  OME_JOB_FAILED = 1,           /* status holds the error; ome_last_error() after poll names it */
+  OME_JOB_REJECTED_MEMORY = 2,
+  OME_JOB_REJECTED_WORK = 3
+} ome_job_outcome;
+typedef struct {
+  int64_t id;
+  int32_t outcome;              /* ome_job_outcome */
+  int32_t status;               /* OME_OK for completed jobs */
+  double arrival_s, admitted_s, done_s;   /* seconds since ome_server_create; admitted_s < 0 if never admitted */
+} ome_server_job;
+typedef struct {
+  int64_t submitted, completed, failed, rejected_memory, rejected_work, queued, running;
+  double p50_ms, p90_ms, p99_ms;          /* latency (arrival to completion seen by poll) of completed jobs */
+  double jobs_per_s, makespan_s;          /* completed / (last completion - first arrival) */
+} ome_serving_stats;
+OME_API int ome_server_create(int device, int32_t n_slots, size_t hbm_budget_bytes, double max_job_work,
+                              ome_server** out);
+/* Queue a job: y <- tree(inputs) of the plan (dxs == NULL), or cost_and_gradient
+ * (dxs[t] receives the gradient of input t; the plan runs unsliced).  inputs,
+ * y and dxs are column-major contiguous device buffers of the plan's dtype;
+ * they and the plan belong to the caller and must stay valid until poll
+ * reports the job.  input_stream (may be NULL): the stream the inputs were
+ * written on; the job's kernels wait for that stream's work at submit time.
+ * work: the job's multiply-adds, for the work cap.  Thread-safe with poll. */
+OME_API int ome_server_submit(ome_server* server, ome_plan* plan, int32_t ninputs, const void* const* inputs,
+                              void* y, void* const* dxs, double work, void* input_stream, int64_t* job_id);
+/* Retire finished jobs, admit queued ones, and return up to max_jobs records
+ * of jobs that finished or were rejected since the last poll (oldest first);
+ * *running = jobs on the device. */
+OME_API int ome_server_poll(ome_server* server, int32_t max_jobs, ome_server_job* jobs, int32_t* n_jobs,
+                            int32_t* running);
+OME_API int ome_server_stats(ome_server* server, ome_serving_stats* stats);
+/* Waits (without a time limit) for every issued job, then frees the slots;
+ * queued jobs are dropped. */
+OME_API int ome_server_destroy(ome_server* server);
+
 /* Allocation-free reduction --------------------------------------------------
  *
  * No counterpart in the reference.  y <- sy*y + sx*sum(x) where every label

@@ -33,8 +33,8 @@ from .core import (AbstractEinsum, DynamicEinCode, DynamicNestedEinsum, EinCode,
                    parse_nested, slice_iterator, uniformsize)
 from .engine import (TropicalTensor, cost_and_gradient, einsum, einsum_, einsum_grad, einsum_many,
                      get_output_array, loop_einsum, loop_einsum_, promote_dtype)
-from .batch import BatchedEinsum, capture_graph
-from .serve import Job, TNServer, pow2_rescale
+from .batch import BatchGraph, BatchedEinsum, capture_graph
+from .serve import Job, NativeTNServer, TNServer, pow2_rescale
 from .distributed import ShardedSlices, allreduce_partial, sharded_einsum, slice_range
 from .autograd import ad_einsum
 from .planner import (GreedyMethod, GreedySlicer, MergeVectors, ScoreFunction, TreeSA, TreeSASlicer,

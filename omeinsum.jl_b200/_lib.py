@@ -25,8 +25,12 @@ EXPORTS = [
     "ome_einsum", "ome_loop_einsum", "ome_einsum_grad", "ome_plan_create", "ome_plan_destroy", "ome_plan_peak_bytes",
     "ome_plan_execute", "ome_plan_gradient", "ome_plan_slice_count", "ome_plan_partial_info",
     "ome_plan_execute_slices", "ome_plan_finish", "ome_reduce_noalloc", "ome_batch_create", "ome_batch_run",
-    "ome_batch_info", "ome_batch_destroy", "ome_treesa", "ome_greedy", "ome_slice_greedy",
+    "ome_batch_info", "ome_batch_destroy", "ome_batch_graph_create", "ome_graph_launch", "ome_graph_destroy",
+    "ome_server_create", "ome_server_submit", "ome_server_poll", "ome_server_stats", "ome_server_destroy",
+    "ome_treesa", "ome_greedy", "ome_slice_greedy",
 ]
+
+JOB_COMPLETED, JOB_FAILED, JOB_REJECTED_MEMORY, JOB_REJECTED_WORK = range(4)
 
 
 class DimensionMismatch(Exception):
@@ -49,6 +53,19 @@ class Tensor(C.Structure):
         ("strides", C.POINTER(C.c_int64)),
         ("labels", C.POINTER(C.c_int32)),
     ]
+
+
+class ServerJob(C.Structure):
+    """ome_server_job"""
+    _fields_ = [("id", C.c_int64), ("outcome", C.c_int32), ("status", C.c_int32), ("arrival_s", C.c_double),
+                ("admitted_s", C.c_double), ("done_s", C.c_double)]
+
+
+class ServingStats(C.Structure):
+    """ome_serving_stats"""
+    _fields_ = [(k, C.c_int64) for k in ("submitted", "completed", "failed", "rejected_memory", "rejected_work",
+                                         "queued", "running")] + \
+               [(k, C.c_double) for k in ("p50_ms", "p90_ms", "p99_ms", "jobs_per_s", "makespan_s")]
 
 
 _lib = None
@@ -101,6 +118,17 @@ def load() -> C.CDLL:
         lib.ome_batch_run.argtypes = [P, P, P, P, P]
         lib.ome_batch_info.argtypes = [P, C.POINTER(C.c_int32), C.POINTER(C.c_float)]
         lib.ome_batch_destroy.argtypes = [P]
+        lib.ome_batch_graph_create.argtypes = [P, P, C.c_int32, C.POINTER(P), C.POINTER(P), C.POINTER(P),
+                                               C.POINTER(P)]
+        lib.ome_graph_launch.argtypes = [P, P]
+        lib.ome_graph_destroy.argtypes = [P]
+        lib.ome_server_create.argtypes = [C.c_int, C.c_int32, C.c_size_t, C.c_double, C.POINTER(P)]
+        lib.ome_server_submit.argtypes = [P, P, C.c_int32, C.POINTER(P), P, C.POINTER(P), C.c_double, P,
+                                          C.POINTER(C.c_int64)]
+        lib.ome_server_poll.argtypes = [P, C.c_int32, C.POINTER(ServerJob), C.POINTER(C.c_int32),
+                                        C.POINTER(C.c_int32)]
+        lib.ome_server_stats.argtypes = [P, C.POINTER(ServingStats)]
+        lib.ome_server_destroy.argtypes = [P]
         lib.ome_reduce_noalloc.argtypes = [P, C.c_int, C.POINTER(Tensor), C.POINTER(Tensor), P, P]
         dp = C.POINTER(C.c_double)
         lib.ome_treesa.argtypes = [C.c_int32, i32p, i32p, C.c_int32, i32p, C.c_int32, dp, i32p, C.c_double,

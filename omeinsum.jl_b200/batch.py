@@ -94,3 +94,46 @@ def capture_graph(fn) -> "torch.cuda.CUDAGraph":
     with torch.cuda.graph(g):
         fn()
     return g
+
+
+class BatchGraph:
+    """A CUDA graph of grouped launches built by the library
+    (``ome_batch_graph_create``): ``BatchGraph([b1, b2])`` captures b1.run()
+    then b2.run() once; ``launch()`` replays them with one call.  The same
+    capture that ``capture_graph`` makes through torch, available to a C or
+    Julia caller of the ABI.  sxs / sys: per batch scalars (default 1, 0)."""
+
+    def __init__(self, batches: Sequence[BatchedEinsum], sxs=None, sys=None):
+        if len(batches) == 0:
+            raise ArgumentError("empty graph")
+        self.batches = list(batches)   # the graph reads their tables and tensors
+        dev = self.batches[0].device
+        self.device = dev
+        n = len(self.batches)
+        hs = (C.c_void_p * n)(*[b.handle.value for b in self.batches])
+        keep = []
+
+        def scal(vals):
+            if vals is None:
+                return None
+            bufs = [_scalar_buf(b.ome, v) for b, v in zip(self.batches, vals)]
+            keep.extend(bufs)
+            return (C.c_void_p * n)(*[C.cast(x, C.c_void_p) for x in bufs])
+
+        g = C.c_void_p()
+        with torch.cuda.device(dev):
+            check(_lib.load().ome_batch_graph_create(self.batches[0].ctx.handle, _stream(dev), n, hs, scal(sxs),
+                                                     scal(sys), C.byref(g)))
+        self.handle = g
+
+    def launch(self):
+        with torch.cuda.device(self.device):
+            check(_lib.load().ome_graph_launch(self.handle, _stream(self.device)))
+        return [b.outputs for b in self.batches]
+
+    def __del__(self):
+        try:
+            if self.handle:
+                _lib.load().ome_graph_destroy(self.handle)
+        except Exception:
+            pass

@@ -217,6 +217,21 @@ int32_t kvec_ok(const void* base, int64_t sk, int64_t s_row, int64_t rows, int64
   return 1;
 }
 
+// Loads the kernel of config cfg (and sets its attributes) without launching it.
+cudaError_t prepare_cfg(ome_dtype dt, int cfg) {
+  if (cfg == CFG_TC) return prepare_group_tc(dt, 3);
+  cudaFuncAttributes fa;
+  cudaError_t e = cudaSuccess;
+  OME_DISPATCH(dt, ALG, {
+    switch (cfg) {
+      case 0: e = cudaFuncGetAttributes(&fa, k_group_gemm<ALG, 32, 32, 2, 2>); break;
+      case 1: e = cudaFuncGetAttributes(&fa, k_group_gemm<ALG, 64, 32, 4, 2>); break;
+      default: e = cudaFuncGetAttributes(&fa, k_group_gemm<ALG, 64, 64, 4, 4>); break;
+    }
+  });
+  return e;
+}
+
 cudaError_t launch_cfg(ome_batch* b, int cfg, const Scalar& sx, const Scalar& sy, cudaStream_t s) {
   const int64_t tiles = b->tiles[cfg];
   if (tiles == 0) return cudaSuccess;
@@ -353,6 +368,69 @@ int ome_batch_info(const ome_batch* b, int32_t* tile_config, float* tuned_us) {
   if (tile_config) *tile_config = b->cfg;
   if (tuned_us)
     for (int c = 0; c < NCFG; ++c) tuned_us[c] = b->tuned_us[c];
+  return OME_OK;
+}
+
+// A CUDA graph of grouped launches, captured on a private stream (the
+// caller's stream is never put in capture mode).
+struct ome_graph {
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+};
+
+int ome_batch_graph_create(ome_ctx* ctx, void* stream, int32_t count, ome_batch* const* batches,
+                           const void* const* sxs, const void* const* sys, ome_graph** out) {
+  if (!ctx || !batches || !out || count < 1) return set_err(OME_INVALID_ARGUMENT, "bad arguments");
+  *out = nullptr;
+  for (int i = 0; i < count; ++i)
+    if (!batches[i]) return set_err(OME_INVALID_ARGUMENT, "NULL batch %d", i);
+  // the batches' tables were uploaded on their creation streams
+  cudaError_t e = cudaStreamSynchronize(static_cast<cudaStream_t>(stream));
+  if (e != cudaSuccess) return cuda_err(e, "graph capture");
+  for (int i = 0; i < count; ++i) {
+    e = prepare_cfg(batches[i]->dt, batches[i]->cfg);
+    if (e != cudaSuccess) return cuda_err(e, "graph capture: loading a kernel");
+  }
+  cudaStream_t cs = nullptr;
+  e = cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking);
+  if (e != cudaSuccess) return cuda_err(e, "graph capture stream");
+  e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
+  cudaError_t le = cudaSuccess;
+  if (e == cudaSuccess) {
+    for (int i = 0; i < count && le == cudaSuccess; ++i) {
+      ome_batch* b = batches[i];
+      const Scalar sx = sxs && sxs[i] ? scalar_from(b->dt, sxs[i]) : scalar_one(b->dt);
+      const Scalar sy = sys && sys[i] ? scalar_from(b->dt, sys[i]) : scalar_zero(b->dt);
+      le = launch_cfg(b, b->cfg, sx, sy, cs);
+    }
+    cudaGraph_t g = nullptr;
+    e = cudaStreamEndCapture(cs, &g);   // always ends the capture
+    auto gr = new ome_graph();
+    gr->graph = g;
+    if (e == cudaSuccess && le == cudaSuccess) e = cudaGraphInstantiate(&gr->exec, g, 0);
+    if (e != cudaSuccess || le != cudaSuccess) {
+      if (gr->exec) cudaGraphExecDestroy(gr->exec);
+      if (g) cudaGraphDestroy(g);
+      delete gr;
+      cudaStreamDestroy(cs);
+      return cuda_err(le != cudaSuccess ? le : e, "graph capture");
+    }
+    *out = gr;
+  }
+  cudaStreamDestroy(cs);
+  return e == cudaSuccess ? OME_OK : cuda_err(e, "graph capture");
+}
+
+int ome_graph_launch(ome_graph* g, void* stream) {
+  if (!g || !g->exec) return set_err(OME_INVALID_ARGUMENT, "NULL graph");
+  return cuda_err(cudaGraphLaunch(g->exec, static_cast<cudaStream_t>(stream)), "graph launch");
+}
+
+int ome_graph_destroy(ome_graph* g) {
+  if (!g) return OME_OK;
+  if (g->exec) cudaGraphExecDestroy(g->exec);
+  if (g->graph) cudaGraphDestroy(g->graph);
+  delete g;
   return OME_OK;
 }
 

@@ -47,4 +47,8 @@ Scalar scalar_one(ome_dtype dt);
 Scalar scalar_zero(ome_dtype dt);
 Scalar scalar_from(ome_dtype dt, const void* p);
 
+// A plan's element type and number of inputs (plan.cu).
+ome_dtype plan_dtype(const ome_plan* p);
+int plan_ninputs(const ome_plan* p);
+
 }  // namespace ome

@@ -2181,6 +2181,26 @@ __device__ __forceinline__ void tmem_ld16_nw(uint32_t taddr, uint32_t (&r)[16]) 
 }
 __device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
 
+// kind::f16 BF16 x BF16 -> F32, K-major A and B, M = 128, N = n (a multiple
+// of 16 up to 256): a tile whose problem ends inside it multiplies only the
+// columns it has.
+__host__ __device__ constexpr uint32_t gt_idesc(uint32_t n) {
+  return (1u << 4) | (1u << 7) | (1u << 10) | ((n >> 3) << 17) | ((uint32_t)(128 >> 4) << 24);
+}
+__device__ __forceinline__ void umma_bf16_i(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t idesc, uint32_t acc) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(d_tmem),
+      "l"(a), "l"(b), "r"(idesc), "r"(acc));
+}
+// Columns of tile nt that hold output (1..128).
+__device__ __forceinline__ int gt_cols(const GtTile* ti) {
+  const int64_t r = ti->p.n - ti->nt * 128;
+  return r < 128 ? (int)r : 128;
+}
+static_assert(gt_idesc(128) == tc::IDESC, "instruction descriptor");
+
 // Scheduler warp: stage every tile of this CTA, in order, in the slot ring.
 __device__ __forceinline__ void gt_scheduler(const GtArgs& t, unsigned char* slots, uint64_t* sched_full,
                                              uint64_t* sched_empty, volatile int* abort_flag, int lane) {
@@ -2230,9 +2250,11 @@ __device__ __forceinline__ void gt_scheduler(const GtArgs& t, unsigned char* slo
 template <bool CPLX> struct GtRegs;
 template <> struct GtRegs<true> {
   float2 a[4], b[8];
+  uint32_t ok;   // bit 0: the A row lies in the problem, bit 1: the B column does
 };
 template <> struct GtRegs<false> {
   float a[16], b[16];
+  uint32_t ok;
 };
 
 // A converter thread's row of A and column of B in the current tile (null
@@ -2299,12 +2321,14 @@ __device__ __forceinline__ void gt_ld8r(const float* row, int64_t sk, int64_t k0
 }
 
 __device__ __forceinline__ void gt_load(const GtRows& w, int kt, int tid, GtRegs<true>& r) {
+  r.ok = (w.a ? 1u : 0u) | (w.b ? 2u : 0u);
   gt_ld4c(w.a, w.ask, (int64_t)kt * 16 + 4 * (tid >> 6), w.K, w.akv, r.a);
 #pragma unroll
   for (int u = 0; u < 2; ++u) gt_ld4c(w.b, w.bsk, (int64_t)kt * 16 + 4 * ((tid >> 7) + 2 * u), w.K, w.bkv, r.b + 4 * u);
 }
 
 __device__ __forceinline__ void gt_load(const GtRows& w, int kt, int tid, GtRegs<false>& r) {
+  r.ok = (w.a ? 1u : 0u) | (w.b ? 2u : 0u);
 #pragma unroll
   for (int u = 0; u < 2; ++u) {
     const int64_t k0 = (int64_t)kt * 32 + 8 * ((tid >> 7) + 2 * u);
@@ -2337,8 +2361,11 @@ __device__ __forceinline__ void gt_store(const GtRegs<true>& r, uint32_t st, int
   // eight distinct bank groups) as pairs (x, y); the other row's pairs are
   // (s y, -s x) with s = +1 for firstp = 1 and -1 for firstp = 0, i.e. the
   // same terms with the sign of one half flipped.
+  // Rows outside the problem are not written: they only reach accumulator
+  // rows and columns that are never stored.
   const int firstp = (lane >> 2) & 1;
   const uint32_t flip = firstp ? 0x80000000u : 0x00008000u;
+  if (r.ok & 1u) {
   uint32_t tx[4][NT], ty[4][NT];
 #pragma unroll
   for (int j = 0; j < 4; ++j) {
@@ -2356,6 +2383,8 @@ __device__ __forceinline__ void gt_store(const GtRegs<true>& r, uint32_t st, int
            make_uint4(pack_hi(ty[0][u], tx[0][u]) ^ flip, pack_hi(ty[1][u], tx[1][u]) ^ flip,
                       pack_hi(ty[2][u], tx[2][u]) ^ flip, pack_hi(ty[3][u], tx[3][u]) ^ flip));
   }
+  }
+  if (!(r.ok & 2u)) return;
   const int nl = tid & 127;
 #pragma unroll
   for (int u = 0; u < 2; ++u) {
@@ -2388,8 +2417,9 @@ __device__ __forceinline__ void gt_store(const GtRegs<false>& r, uint32_t st, in
       va[j] = r.a[8 * u + j];
       vb[j] = r.b[8 * u + j];
     }
-    split8_store<NT>(va, st + so);
-    split8_store<NT>(vb, st + gt::Cfg<NT>::STAGE_BYTES / 2 + so);
+    // rows outside the problem only reach discarded accumulator rows / columns
+    if (r.ok & 1u) split8_store<NT>(va, st + so);
+    if (r.ok & 2u) split8_store<NT>(vb, st + gt::Cfg<NT>::STAGE_BYTES / 2 + so);
   }
 }
 
@@ -2572,13 +2602,14 @@ __device__ __forceinline__ void gt_drain(const GtArgs& t, float* acc, uint32_t t
     if (!__all_sync(0xffffffffu, mbar_wait(&sched_full[ss], (j / NSLOT) & 1, abort_flag))) return;
     const GtTile* ti = reinterpret_cast<const GtTile*>(slots + ss * SLOT_BYTES);
     const int nch = (gt_stages<CPLX>(ti->p) + CHUNK - 1) / CHUNK;
+    const int ngrp = (gt_cols(ti) + 15) >> 4;   // 16-column groups that hold output
     for (int ci = 0; ci < nch; ++ci, ++gc) {
       const int b = gc & 1;
       if (!__all_sync(0xffffffffu, mbar_wait(&chunk_done[b], (gc >> 1) & 1, abort_flag))) return;
       tc_fence_after();
       const bool last = ci + 1 == nch;
 #pragma unroll 1
-      for (int hh = 0; hh < 8; ++hh) {
+      for (int hh = 0; hh < ngrp; ++hh) {
         uint32_t rm[16], rc[16];
         const uint32_t col = (uint32_t)(16 * hh);
         tmem_ld16_nw(tmem + (uint32_t)(256 * b) + lane_off + col, rm);
@@ -2603,7 +2634,7 @@ __device__ __forceinline__ void gt_drain(const GtArgs& t, float* acc, uint32_t t
 #pragma unroll
       for (int jj = 0; jj < 16; ++jj) v[jj] = 0.f;
 #pragma unroll 1
-      for (int hh = 0; hh < 8; ++hh) gt_store_cols<CPLX>(t, ti, row, 16 * hh, v);
+      for (int hh = 0; hh < ngrp; ++hh) gt_store_cols<CPLX>(t, ti, row, 16 * hh, v);
     }
     __syncwarp();
     if (lane == 0) mbar_arrive(&sched_empty[ss]);
@@ -2673,7 +2704,9 @@ __global__ void __launch_bounds__(gt::NTHREADS, 1) k_group_tc(const __grid_const
     for (int64_t tile = blockIdx.x; tile < t.tiles && ok; tile += gridDim.x, ++j) {
       const int ss = j % NSLOT;
       if (!mbar_wait(&sched_full[ss], (j / NSLOT) & 1, abort_flag)) break;
-      const int nkt = gt_stages<CPLX>(reinterpret_cast<const GtTile*>(slots + ss * SLOT_BYTES)->p);
+      const GtTile* ti = reinterpret_cast<const GtTile*>(slots + ss * SLOT_BYTES);
+      const int nkt = gt_stages<CPLX>(ti->p);
+      const uint32_t idesc = gt_idesc((uint32_t)((gt_cols(ti) + 15) & ~15));
       mbar_arrive(&sched_empty[ss]);
       for (int kt = 0; kt < nkt; ++kt, ++it) {
         const uint32_t c = gc + kt / CHUNK;
@@ -2694,13 +2727,13 @@ __global__ void __launch_bounds__(gt::NTHREADS, 1) k_group_tc(const __grid_const
             bdsc[u] = umma_desc(sb + (NT + u) * TILE_BYTES + off);
           }
           const uint32_t keep = (first && kk == 0) ? 0u : 1u;
-          umma_bf16(tmem + (uint32_t)(256 * b), ad[0], bdsc[0], keep);
+          umma_bf16_i(tmem + (uint32_t)(256 * b), ad[0], bdsc[0], idesc, keep);
           bool first_cross = true;
 #pragma unroll
           for (int d = 1; d < NT; ++d)
 #pragma unroll
             for (int i = 0; i <= d; ++i) {
-              umma_bf16(tmem + (uint32_t)(256 * b + 128), ad[i], bdsc[d - i], first_cross ? keep : 1u);
+              umma_bf16_i(tmem + (uint32_t)(256 * b + 128), ad[i], bdsc[d - i], idesc, first_cross ? keep : 1u);
               first_cross = false;
             }
         }
@@ -2722,7 +2755,7 @@ __global__ void __launch_bounds__(gt::NTHREADS, 1) k_group_tc(const __grid_const
 
 namespace {
 template <int NT, bool CPLX>
-cudaError_t launch_gt(const GtArgs& t, int grid, cudaStream_t s) {
+cudaError_t prepare_gt() {
   static bool attr = false;
   if (!attr) {
     cudaError_t e = cudaFuncSetAttribute(k_group_tc<NT, CPLX>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -2730,10 +2763,22 @@ cudaError_t launch_gt(const GtArgs& t, int grid, cudaStream_t s) {
     if (e != cudaSuccess) return e;
     attr = true;
   }
+  return cudaSuccess;
+}
+template <int NT, bool CPLX>
+cudaError_t launch_gt(const GtArgs& t, int grid, cudaStream_t s) {
+  const cudaError_t e = prepare_gt<NT, CPLX>();
+  if (e != cudaSuccess) return e;
   k_group_tc<NT, CPLX><<<grid, gt::NTHREADS, gt::Cfg<NT>::SMEM_BYTES, s>>>(t);
   return cudaGetLastError();
 }
 }  // namespace
+
+cudaError_t prepare_group_tc(ome_dtype dt, int nterms) {
+  if ((dt != OME_F32 && dt != OME_C32) || (nterms != 2 && nterms != 3)) return cudaErrorNotSupported;
+  if (dt == OME_C32) return nterms == 3 ? prepare_gt<3, true>() : prepare_gt<2, true>();
+  return nterms == 3 ? prepare_gt<3, false>() : prepare_gt<2, false>();
+}
 
 cudaError_t launch_group_tc(ome_dtype dt, int nterms, const GroupProblem* probs, const int32_t* tile_prob, int nprob,
                             int64_t tiles, int grid, const Scalar& sx, const Scalar& sy, int sy_zero, int sx_one,

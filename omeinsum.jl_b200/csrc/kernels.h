@@ -135,6 +135,9 @@ struct GroupProblem {
 // embedding): 128 x 128 tiles of the (embedded) output, BF16 split products
 // (nterms 2 or 3) formed in shared memory; tiles_m counts 128 real rows
 // (64 complex rows for C32).  cudaErrorNotSupported for other dtypes.
+// Sets the kernel's shared-memory attribute (and so loads it); done by the
+// first launch, and before a graph capture so that none happens inside it.
+cudaError_t prepare_group_tc(ome_dtype dt, int nterms);
 // tile_prob[t] is the problem that owns global tile t.
 cudaError_t launch_group_tc(ome_dtype dt, int nterms, const GroupProblem* probs, const int32_t* tile_prob, int nprob,
                             int64_t tiles, int grid, const Scalar& sx, const Scalar& sy, int sy_zero, int sx_one,

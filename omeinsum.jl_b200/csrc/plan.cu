@@ -575,6 +575,8 @@ int ome_plan_finish(ome_ctx* ctx, ome_plan* p, void* stream, const void* partial
 namespace ome {
 cudaError_t launch_conj(ome_dtype dt, void* x, int64_t n, cudaStream_t s);
 cudaError_t launch_fill_one(ome_dtype dt, void* x, int64_t n, cudaStream_t s);
+ome_dtype plan_dtype(const ome_plan* p) { return p->dt; }
+int plan_ninputs(const ome_plan* p) { return p->ninputs; }
 }
 
 extern "C" {

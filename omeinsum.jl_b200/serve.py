@@ -90,6 +90,15 @@ class Job:
         return self.done - self.arrival
 
 
+def job_work(job: Job) -> float:
+    """Multiply-adds of the job's tree (gradient jobs: three forward passes)."""
+    if job._work is None:
+        from .planner import contraction_complexity
+        sd = get_size_dict(job.code.getixsv(), job.xs)
+        job._work = 2.0 ** contraction_complexity(job.code, sd).tc * (3.0 if job.grad else 1.0)
+    return job._work
+
+
 class _Slot:
     """One admission slot: a stream, a context, and a host thread that issues
     the slot's job (a big job's kernel issue must not block the others)."""
@@ -167,12 +176,7 @@ class TNServer:
         return p, [_f_contig(t) for t in ts], sd, plan, need
 
     def _work(self, job: Job) -> float:
-        """Multiply-adds of the job's tree (gradient jobs: three forward passes)."""
-        if job._work is None:
-            from .planner import contraction_complexity
-            sd = get_size_dict(job.code.getixsv(), job.xs)
-            job._work = 2.0 ** contraction_complexity(job.code, sd).tc * (3.0 if job.grad else 1.0)
-        return job._work
+        return job_work(job)
 
     def _launch(self, slot: _Slot, job: Job, prepared):
         """Reserve the slot and hand the job's kernel issue to the slot's thread."""
@@ -356,3 +360,104 @@ class TNServer:
                 "rejected_over_work_cap": sum(1 for j in self.rejected if j.reject_reason == "work"),
                 "p50_ms": float(np.percentile(lat, 50) * 1e3), "p99_ms": float(np.percentile(lat, 99) * 1e3),
                 "jobs_per_s": len(self.finished) / span if span > 0 else 0.0, "makespan_s": span}
+
+
+class NativeTNServer:
+    """The same serving loop inside the library (``ome_server_*`` in
+    include/ome_b200.h): slots, issue threads, admission by planned peak
+    bytes, exclusive runs of jobs above a slot's share and the work cap are
+    C++; Python only plans jobs, allocates their outputs and polls.  This is
+    the interface a Julia service binds (no Python on its path); ``TNServer``
+    above is the Python rendering of the same rules."""
+
+    def __init__(self, n_slots: int = 8, hbm_budget_bytes: float = 150e9, device: int = 0, prec: int = 0,
+                 max_job_flops: Optional[float] = None):
+        self.device = torch.device("cuda", device)
+        self.prec = prec
+        self.max_job_flops = max_job_flops
+        h = C.c_void_p()
+        check(_lib.load().ome_server_create(device, n_slots, int(hbm_budget_bytes),
+                                            float(max_job_flops or 0.0), C.byref(h)))
+        self.handle = h
+        self._live = {}            # job id -> (job, buffers the library reads or writes)
+        self.finished: List[Job] = []
+        self.rejected: List[Job] = []
+
+    def submit(self, job: Job) -> int:
+        """Plan the job, allocate its outputs and queue it; inputs written on
+        the current stream are waited for by the job's kernels."""
+        p = _Prepared(job.xs)
+        ts = [_f_contig(t) for t in p.tensors]
+        sd = get_size_dict(job.code.getixsv(), ts)
+        code = job.code
+        if job.grad and isinstance(code, SlicedEinsum):
+            code = code.eins   # gradients run unsliced, as the reference does (src/bp.jl:26-28)
+        plan = get_plan(code, sd, p.ome, self.prec)
+        ne = code.eins if isinstance(code, SlicedEinsum) else code
+        y = _alloc([sd[l] for l in ne.eins.iy], p.dtype, self.device)
+        ptrs = (C.c_void_p * len(ts))(*[t.data_ptr() for t in ts])
+        dxs = dptr = None
+        if job.grad:
+            dxs = [_alloc(t.shape, p.dtype, self.device) for t in ts]
+            dptr = (C.c_void_p * len(dxs))(*[d.data_ptr() for d in dxs])
+        work = job_work(job) if self.max_job_flops is not None else 0.0
+        jid = C.c_int64()
+        check(_lib.load().ome_server_submit(self.handle, plan.handle, len(ts), ptrs, y.data_ptr(), dptr, work,
+                                            C.c_void_p(torch.cuda.current_stream(self.device).cuda_stream),
+                                            C.byref(jid)))
+        job.id = jid.value
+        job.value, job.grads = y, dxs
+        self._live[job.id] = (job, (plan, ts, ptrs, y, dxs, dptr))
+        return job.id
+
+    def poll(self) -> int:
+        """Retire finished jobs and admit queued ones; returns the number running."""
+        recs = (_lib.ServerJob * 64)()
+        n, running = C.c_int32(), C.c_int32()
+        while True:
+            check(_lib.load().ome_server_poll(self.handle, 64, recs, C.byref(n), C.byref(running)))
+            for r in recs[:n.value]:
+                job, _ = self._live.pop(r.id)
+                job.arrival, job.admitted, job.done = r.arrival_s, r.admitted_s, r.done_s
+                if r.outcome == _lib.JOB_COMPLETED:
+                    self.finished.append(job)
+                else:
+                    job.reject_reason = {_lib.JOB_REJECTED_MEMORY: "memory", _lib.JOB_REJECTED_WORK: "work"}.get(
+                        r.outcome, "failed")
+                    job.value = job.grads = None
+                    self.rejected.append(job)
+            if n.value < 64:
+                return running.value
+
+    def run_trace(self, jobs: Sequence[Job], timeout_s: float = 600.0):
+        """Submit jobs at their arrival times (seconds from now) and poll until
+        all have finished; returns the library's statistics."""
+        pending = deque(sorted(jobs, key=lambda j: j.arrival))
+        t0 = time.perf_counter()
+        while pending or self._live:
+            now = time.perf_counter() - t0
+            while pending and pending[0].arrival <= now:
+                self.submit(pending.popleft())
+            self.poll()
+            if now > timeout_s:
+                break
+            time.sleep(0.0002)
+        return self.stats()
+
+    def stats(self):
+        st = _lib.ServingStats()
+        check(_lib.load().ome_server_stats(self.handle, C.byref(st)))
+        return {k: getattr(st, k) for k, _ in _lib.ServingStats._fields_}
+
+    def close(self):
+        """Wait for every issued job and free the slots (queued jobs are dropped)."""
+        if self.handle:
+            _lib.load().ome_server_destroy(self.handle)
+            self.handle = None
+        self._live.clear()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
