@@ -564,6 +564,32 @@ def serve_section(ome, dev, njobs=400, rate=2000.0, seed=10, nmin=40, nmax=200, 
         ref = float(ref.double().cpu()) * 2.0 ** lg
         if ref != 0 and math.isfinite(ref):
             errs.append(abs(j.scalar() - ref) / abs(ref))
+    # the same stream through the library's own serving loop (ome_server_*):
+    # admission, slots and issue threads in C++, the same rules
+    ome.release_workspaces()
+    torch.cuda.empty_cache()
+    nsrv = ome.NativeTNServer(n_slots=16, hbm_budget_bytes=150e9, max_job_flops=work_cap)
+    nsrv.run_trace([ome.Job(j.code, j.xs, grad=j.grad, arrival=j.arrival, log2_scale=j.log2_scale)
+                    for j in jobs[:48]], timeout_s=cap_s)
+    njobs_native = [ome.Job(j.code, j.xs, grad=j.grad, arrival=j.arrival, log2_scale=j.log2_scale) for j in jobs]
+    nsrv.finished, nsrv.rejected = [], []
+    t_native = time.perf_counter()
+    nsrv.run_trace(njobs_native, timeout_s=cap_s)
+    nsrv.close()
+    ndone = {id(j) for j in nsrv.finished}
+    both = [(a, b) for a, b in zip(jobs, njobs_native) if id(a) in finished_ids and id(b) in ndone]
+    same = sum(1 for a, b in both if torch.equal(a.value, b.value))
+    nlat = np.array([j.done - j.arrival for j in nsrv.finished]) if nsrv.finished else np.zeros(1)
+    reasons = [j.reject_reason for j in nsrv.rejected]   # this stream only (the library counts both passes)
+    native = {"completed": len(nsrv.finished), "rejected_over_work_cap": reasons.count("work"),
+              "rejected_memory": reasons.count("memory"), "failed": reasons.count("failed"),
+              "p50_ms": float(np.percentile(nlat, 50) * 1e3), "p90_ms": float(np.percentile(nlat, 90) * 1e3),
+              "p99_ms": float(np.percentile(nlat, 99) * 1e3),
+              "jobs_per_s": len(nsrv.finished) / max(max((j.done for j in nsrv.finished), default=0.0)
+                                                     - min((j.arrival for j in nsrv.finished), default=0.0), 1e-9),
+              "wall_s": time.perf_counter() - t_native,
+              "values_identical_to_python_server": f"{same}/{len(both)}",
+              "api": "ome_server_create/submit/poll/stats (C ABI), driven by NativeTNServer"}
     lat = np.array([j.latency for j in done]) if done else np.zeros(1)
     st.update({"workload": f"{njobs} jobs, Poisson {rate:.0f}/s (seed {seed}), n uniform even [{nmin},{nmax}], "
                            "bond 2, unscaled FP32 normal(0,1), 10% gradient jobs, greedy order (best of 10) + greedy "
@@ -582,7 +608,7 @@ def serve_section(ome, dev, njobs=400, rate=2000.0, seed=10, nmin=40, nmax=200, 
                                    "within_1e-5": sum(e <= 1e-5 for e in errs),
                                    "reference": "FP64 evaluation of the same tree by the library (cheapest jobs "
                                                 f"first, {ref_cap_s:.0f} s cap)"},
-               "client_planning_s": plan_s})
+               "client_planning_s": plan_s, "native_server": native})
     return st
 
 
@@ -615,7 +641,7 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--prec", type=int, default=0, help="0 AUTO (BF16x3), 1 plain FP32")
+    ap.add_argument("--prec", type=int, default=0, help="0 AUTO (BF16x6), 1 plain FP32, 2 BF16x3, 3 BF16x6")
     ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline leg")
     ap.add_argument("--no-tn", action="store_true", help="skip the tensor-network precision section")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched MPS-transfer section")

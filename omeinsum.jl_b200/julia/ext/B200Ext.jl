@@ -305,6 +305,87 @@ function b200_cost_and_gradient(code, xs, dy = nothing)
     return y, dxs
 end
 
+# ---------------------------------------------------------------------------
+# Serving through the library's own loop (ome_server_*): a Julia service
+# submits whole trees and polls; slots, admission and issue threads are C++.
+
+struct OmeServerJob        # ome_server_job
+    id::Int64
+    outcome::Int32         # 0 completed, 1 failed, 2 rejected (memory), 3 rejected (work cap)
+    status::Int32
+    arrival_s::Float64
+    admitted_s::Float64
+    done_s::Float64
+end
+
+mutable struct B200Server
+    handle::Ptr{Cvoid}
+    live::Dict{Int64,Any}  # job id -> the arrays the library reads or writes until poll reports it
+end
+
+"""B200Server(; slots, budget_bytes, max_work): a serving loop on the current
+device; jobs above a slot's share run alone, jobs above the budget or the work
+cap are rejected at admission."""
+function B200Server(; slots::Integer = 8, budget_bytes::Integer = 150 * 10^9, max_work::Real = 0)
+    r = Ref{Ptr{Cvoid}}(C_NULL)
+    check(@ccall $(sym(:ome_server_create))(CUDA.deviceid(CUDA.device())::Cint, Int32(slots)::Int32,
+                                            Csize_t(budget_bytes)::Csize_t, Float64(max_work)::Float64,
+                                            r::Ref{Ptr{Cvoid}})::Cint)
+    srv = B200Server(r[], Dict{Int64,Any}())
+    finalizer(close, srv)
+    return srv
+end
+
+"""submit!(srv, code, xs; grad = false) -> (id, y, dxs): queue the tree's value
+(or cost_and_gradient, unsliced as src/bp.jl:26-28) on the server; y and dxs
+are filled when poll! reports the job."""
+function submit!(srv::B200Server, code, xs; grad::Bool = false, work::Real = 0)
+    ne0 = code isa SlicedEinsum ? code.eins : code
+    size_dict = OMEinsum.get_size_dict!(getixsv(ne0), xs, Dict{OMEinsum.labeltype(ne0),Int}())
+    T = promote_type(map(eltype, xs)...)
+    tree = grad ? ne0 : code
+    p = plan(tree, size_dict, T)
+    ins = map(x -> dense(T, x), xs)
+    y = CuArray{T}(undef, map(l -> size_dict[l], getiyv(ne0))...)
+    dxs = grad ? map(x -> CuArray{T}(undef, size(x)...), ins) : nothing
+    ptrs = Ptr{Cvoid}[reinterpret(Ptr{Cvoid}, pointer(x)) for x in ins]
+    gptrs = grad ? Ptr{Cvoid}[reinterpret(Ptr{Cvoid}, pointer(g)) for g in dxs] : Ptr{Cvoid}[]
+    id = Ref{Int64}(0)
+    GC.@preserve ptrs gptrs begin
+        check(@ccall $(sym(:ome_server_submit))(srv.handle::Ptr{Cvoid}, p::Ptr{Cvoid}, Int32(length(ins))::Int32,
+                                                ptrs::Ptr{Ptr{Cvoid}}, reinterpret(Ptr{Cvoid}, pointer(y))::Ptr{Cvoid},
+                                                (grad ? pointer(gptrs) : C_NULL)::Ptr{Ptr{Cvoid}}, Float64(work)::Float64,
+                                                stream()::Ptr{Cvoid}, id::Ref{Int64})::Cint)
+    end
+    srv.live[id[]] = (ins, y, dxs)
+    return id[], y, dxs
+end
+
+"""poll!(srv) -> (records, running): retire finished jobs, admit queued ones."""
+function poll!(srv::B200Server)
+    recs = Vector{OmeServerJob}(undef, 64)
+    n, running = Ref{Int32}(0), Ref{Int32}(0)
+    out = OmeServerJob[]
+    while true
+        check(@ccall $(sym(:ome_server_poll))(srv.handle::Ptr{Cvoid}, Int32(64)::Int32, recs::Ptr{OmeServerJob},
+                                              n::Ref{Int32}, running::Ref{Int32})::Cint)
+        for r in view(recs, 1:n[])
+            delete!(srv.live, r.id)
+            push!(out, r)
+        end
+        n[] < 64 && return out, Int(running[])
+    end
+end
+
+function Base.close(srv::B200Server)
+    if srv.handle != C_NULL
+        @ccall $(sym(:ome_server_destroy))(srv.handle::Ptr{Cvoid})::Cint
+        srv.handle = C_NULL
+        empty!(srv.live)
+    end
+    return nothing
+end
+
 """Synchronise the stream and raise if a bounded device-side wait gave up."""
 device_status() = check(@ccall $(sym(:ome_device_status))(stream()::Ptr{Cvoid})::Cint)
 
