@@ -3,6 +3,7 @@
 // OMEinsum.jl (src/Core.jl:116-145 EinIndexer: offset = sum (i_d-1)*stride_d).
 #pragma once
 
+#include <atomic>
 #include <utility>
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -167,6 +168,21 @@ inline size_t dtype_size(ome_dtype d) {
   }
 
 // 16 raw bytes holding one scalar of any dtype (sx, sy).
+// Raises kernel's dynamic shared-memory limit to `bytes` once per device
+// (the attribute belongs to the device's context), safely from any host
+// thread; `done` records the devices already set (bit = device ordinal).
+template <class K>
+inline cudaError_t set_smem_once(std::atomic<unsigned long long>& done, K* kernel, int bytes) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  const unsigned long long bit = 1ull << (dev & 63);
+  if (done.load(std::memory_order_acquire) & bit) return cudaSuccess;
+  e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  if (e == cudaSuccess) done.fetch_or(bit, std::memory_order_release);
+  return e;
+}
+
 struct Scalar {
   alignas(16) unsigned char b[16];
 };

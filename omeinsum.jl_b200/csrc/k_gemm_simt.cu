@@ -420,15 +420,10 @@ template <class A, int NS>
 static cudaError_t launch_gemm_bstage_t(const GemmArgs& g, cudaStream_t s) {
   using Cf = BsCfg<NS>;
   const size_t smem = (size_t)Cf::ELEMS * sizeof(typename A::T);
-  static bool attr = false;
-  if (!attr) {
-    cudaError_t e =
-        cudaFuncSetAttribute(k_gemm_bstage<A, true, NS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e == cudaSuccess)
-      e = cudaFuncSetAttribute(k_gemm_bstage<A, false, NS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return e;
-    attr = true;
-  }
+  static std::atomic<unsigned long long> attr_full{0}, attr_part{0};
+  cudaError_t e = set_smem_once(attr_full, k_gemm_bstage<A, true, NS>, (int)smem);
+  if (e == cudaSuccess) e = set_smem_once(attr_part, k_gemm_bstage<A, false, NS>, (int)smem);
+  if (e != cudaSuccess) return e;
   const dim3 grid((unsigned)((g.L + Cf::NB - 1) / Cf::NB), (unsigned)((g.N + NS - 1) / NS));
   const bool full = g.M == Cf::MT && g.N % NS == 0 && g.K % Cf::KC == 0 && g.L % Cf::NB == 0;
   if (full) k_gemm_bstage<A, true, NS><<<grid, Cf::NT, smem, s>>>(g);

@@ -505,14 +505,11 @@ cudaError_t launch_gemm_split(const GemmArgs& g, int nterms, void* workspace, si
                               cudaStream_t s) {
   using namespace tc;
   if (!gemm_split_supported(g) || (nterms != 2 && nterms != 3)) return cudaErrorNotSupported;
-  static bool attr_set[2] = {false, false};
-  if (!attr_set[nterms - 2]) {
-    cudaError_t e = nterms == 2 ? cudaFuncSetAttribute(k_gemm_bf16x3<2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                       Cfg<2>::SMEM_BYTES)
-                                : cudaFuncSetAttribute(k_gemm_bf16x3<3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                       Cfg<3>::SMEM_BYTES);
+  static std::atomic<unsigned long long> attr2{0}, attr3{0};
+  {
+    const cudaError_t e = nterms == 2 ? set_smem_once(attr2, k_gemm_bf16x3<2>, Cfg<2>::SMEM_BYTES)
+                                      : set_smem_once(attr3, k_gemm_bf16x3<3>, Cfg<3>::SMEM_BYTES);
     if (e != cudaSuccess) return e;
-    attr_set[nterms - 2] = true;
   }
   TcArgs t;
   memset(&t, 0, sizeof(t));
@@ -948,14 +945,11 @@ cudaError_t launch_gemm_packed(const GemmArgs& g, int nterms, void* workspace, s
                                cudaStream_t s, int64_t* ctab) {
   using namespace pk;
   if (!gemm_split_supported(g) || (nterms != 2 && nterms != 3)) return cudaErrorNotSupported;
-  static bool attr_set[2] = {false, false};
-  if (!attr_set[nterms - 2]) {
-    cudaError_t e = nterms == 2 ? cudaFuncSetAttribute(k_gemm_packed<2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                       Cfg<2>::SMEM_BYTES)
-                                : cudaFuncSetAttribute(k_gemm_packed<3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                       Cfg<3>::SMEM_BYTES);
+  static std::atomic<unsigned long long> attr2{0}, attr3{0};
+  {
+    const cudaError_t e = nterms == 2 ? set_smem_once(attr2, k_gemm_packed<2>, Cfg<2>::SMEM_BYTES)
+                                      : set_smem_once(attr3, k_gemm_packed<3>, Cfg<3>::SMEM_BYTES);
     if (e != cudaSuccess) return e;
-    attr_set[nterms - 2] = true;
   }
   const int64_t TM = (g.M + BM - 1) / BM, TN = (g.N + BN - 1) / BN, NKT = (g.K + BK - 1) / BK;
   const size_t blob = (size_t)nterms * TILE_BYTES;
@@ -1705,13 +1699,9 @@ bool make_operand_map(CUtensorMap* map, const void* base, int64_t R, int64_t K, 
 
 template <int NT, bool AK, bool BKM>
 cudaError_t launch_t2(const T2Args& t, const CUtensorMap& ma, const CUtensorMap& mb, int grid, cudaStream_t s) {
-  static bool attr = false;
-  if (!attr) {
-    cudaError_t e = cudaFuncSetAttribute(k_gemm_tma2<NT, AK, BKM>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         t2::Cfg<NT>::SMEM_BYTES);
-    if (e != cudaSuccess) return e;
-    attr = true;
-  }
+  static std::atomic<unsigned long long> attr{0};
+  const cudaError_t e = set_smem_once(attr, k_gemm_tma2<NT, AK, BKM>, t2::Cfg<NT>::SMEM_BYTES);
+  if (e != cudaSuccess) return e;
   k_gemm_tma2<NT, AK, BKM><<<grid, t2::NTHREADS, t2::Cfg<NT>::SMEM_BYTES, s>>>(t, ma, mb);
   return cudaGetLastError();
 }
@@ -2082,16 +2072,10 @@ cudaError_t launch_gemm_bdiag(const GemmArgs& g, int nterms, cudaStream_t s) {
   t.nk = (int)((g.K + bd::BK - 1) / bd::BK);
   t.c_max = (g.L - 1) + (g.M - 1) * g.m_sc[0] + (g.N - 1) * g.n_sc[0];
   const unsigned grid = (unsigned)((g.L + bd::NB - 1) / bd::NB);
-  static bool attr[2] = {false, false};
-  cudaError_t e = cudaSuccess;
-  if (!attr[nterms - 2]) {
-    e = nterms == 3 ? cudaFuncSetAttribute(k_gemm_bdiag<3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                           bd::Cfg<3>::SMEM_BYTES)
-                    : cudaFuncSetAttribute(k_gemm_bdiag<2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                           bd::Cfg<2>::SMEM_BYTES);
-    if (e != cudaSuccess) return e;
-    attr[nterms - 2] = true;
-  }
+  static std::atomic<unsigned long long> attr2{0}, attr3{0};
+  cudaError_t e = nterms == 3 ? set_smem_once(attr3, k_gemm_bdiag<3>, bd::Cfg<3>::SMEM_BYTES)
+                              : set_smem_once(attr2, k_gemm_bdiag<2>, bd::Cfg<2>::SMEM_BYTES);
+  if (e != cudaSuccess) return e;
   {
     KernelTimer kt(s, "k_gemm_bdiag");
     if (nterms == 3) k_gemm_bdiag<3><<<grid, bd::NTHREADS, bd::Cfg<3>::SMEM_BYTES, s>>>(t, ma, mb);
@@ -2756,14 +2740,8 @@ __global__ void __launch_bounds__(gt::NTHREADS, 1) k_group_tc(const __grid_const
 namespace {
 template <int NT, bool CPLX>
 cudaError_t prepare_gt() {
-  static bool attr = false;
-  if (!attr) {
-    cudaError_t e = cudaFuncSetAttribute(k_group_tc<NT, CPLX>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         gt::Cfg<NT>::SMEM_BYTES);
-    if (e != cudaSuccess) return e;
-    attr = true;
-  }
-  return cudaSuccess;
+  static std::atomic<unsigned long long> attr{0};
+  return set_smem_once(attr, k_group_tc<NT, CPLX>, gt::Cfg<NT>::SMEM_BYTES);
 }
 template <int NT, bool CPLX>
 cudaError_t launch_gt(const GtArgs& t, int grid, cudaStream_t s) {
