@@ -364,6 +364,9 @@ OME_API int ome_server_submit(ome_server* server, ome_plan* plan, int32_t ninput
 OME_API int ome_server_poll(ome_server* server, int32_t max_jobs, ome_server_job* jobs, int32_t* n_jobs,
                             int32_t* running);
 OME_API int ome_server_stats(ome_server* server, ome_serving_stats* stats);
+/* The server's clock: seconds since ome_server_create (the time base of
+ * ome_server_job), for callers that account latency from their own arrivals. */
+OME_API int ome_server_clock(const ome_server* server, double* seconds);
 /* Waits (without a time limit) for every issued job, then frees the slots;
  * queued jobs are dropped. */
 OME_API int ome_server_destroy(ome_server* server);

@@ -26,7 +26,7 @@ EXPORTS = [
     "ome_plan_execute", "ome_plan_gradient", "ome_plan_slice_count", "ome_plan_partial_info",
     "ome_plan_execute_slices", "ome_plan_finish", "ome_reduce_noalloc", "ome_batch_create", "ome_batch_run",
     "ome_batch_info", "ome_batch_destroy", "ome_batch_graph_create", "ome_graph_launch", "ome_graph_destroy",
-    "ome_server_create", "ome_server_submit", "ome_server_poll", "ome_server_stats", "ome_server_destroy",
+    "ome_server_create", "ome_server_submit", "ome_server_poll", "ome_server_stats", "ome_server_clock", "ome_server_destroy",
     "ome_treesa", "ome_greedy", "ome_slice_greedy",
 ]
 
@@ -128,6 +128,7 @@ def load() -> C.CDLL:
         lib.ome_server_poll.argtypes = [P, C.c_int32, C.POINTER(ServerJob), C.POINTER(C.c_int32),
                                         C.POINTER(C.c_int32)]
         lib.ome_server_stats.argtypes = [P, C.POINTER(ServingStats)]
+        lib.ome_server_clock.argtypes = [P, C.POINTER(C.c_double)]
         lib.ome_server_destroy.argtypes = [P]
         lib.ome_reduce_noalloc.argtypes = [P, C.c_int, C.POINTER(Tensor), C.POINTER(Tensor), P, P]
         dp = C.POINTER(C.c_double)

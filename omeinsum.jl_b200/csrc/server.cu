@@ -395,6 +395,12 @@ int ome_server_stats(ome_server* s, ome_serving_stats* st) {
   return OME_OK;
 }
 
+int ome_server_clock(const ome_server* s, double* seconds) {
+  if (!s || !seconds) return set_err(OME_INVALID_ARGUMENT, "NULL argument");
+  *seconds = s->clock();
+  return OME_OK;
+}
+
 int ome_server_destroy(ome_server* s) {
   if (!s) return OME_OK;
   DeviceScope ds(s->device);

@@ -382,6 +382,7 @@ class NativeTNServer:
         self._live = {}            # job id -> (job, buffers the library reads or writes)
         self.finished: List[Job] = []
         self.rejected: List[Job] = []
+        self._t0 = None            # server clock at the start of run_trace (None: report the library's times)
 
     def submit(self, job: Job) -> int:
         """Plan the job, allocate its outputs and queue it; inputs written on
@@ -418,7 +419,10 @@ class NativeTNServer:
             check(_lib.load().ome_server_poll(self.handle, 64, recs, C.byref(n), C.byref(running)))
             for r in recs[:n.value]:
                 job, _ = self._live.pop(r.id)
-                job.arrival, job.admitted, job.done = r.arrival_s, r.admitted_s, r.done_s
+                if self._t0 is None:
+                    job.arrival, job.admitted, job.done = r.arrival_s, r.admitted_s, r.done_s
+                else:   # trace time: latency from the job's nominal arrival, as TNServer reports it
+                    job.admitted, job.done = r.admitted_s - self._t0, r.done_s - self._t0
                 if r.outcome == _lib.JOB_COMPLETED:
                     self.finished.append(job)
                 else:
@@ -431,17 +435,26 @@ class NativeTNServer:
 
     def run_trace(self, jobs: Sequence[Job], timeout_s: float = 600.0):
         """Submit jobs at their arrival times (seconds from now) and poll until
-        all have finished; returns the library's statistics."""
+        all have finished; job times are then seconds from the trace start,
+        and latency runs from each job's nominal arrival.  Returns the
+        library's counters (which also cover earlier traces)."""
         pending = deque(sorted(jobs, key=lambda j: j.arrival))
+        c = C.c_double()
+        check(_lib.load().ome_server_clock(self.handle, C.byref(c)))
+        self._t0 = c.value
         t0 = time.perf_counter()
-        while pending or self._live:
-            now = time.perf_counter() - t0
-            while pending and pending[0].arrival <= now:
-                self.submit(pending.popleft())
-            self.poll()
-            if now > timeout_s:
-                break
-            time.sleep(0.0002)
+        try:
+            while pending or self._live:
+                now = time.perf_counter() - t0
+                while pending and pending[0].arrival <= now:
+                    self.submit(pending.popleft())
+                    self.poll()   # admission keeps up while a burst of arrivals is planned
+                self.poll()
+                if now > timeout_s:
+                    break
+                time.sleep(0.0002)
+        finally:
+            self._t0 = None
         return self.stats()
 
     def stats(self):
