@@ -903,6 +903,11 @@ struct TransArgs {
   FastDiv t0, tt;
   FastDiv bdiv[MAXM];
   int32_t bxs[MAXM], bys[MAXM];
+  // k_transpose_v4 only: pa_shift > 0 when the tile's x-fast index runs over
+  // two modes adjacent in x (x's contiguous mode of extent 2^pa_shift and the
+  // next one), so that x rows are 256 bytes long although x's contiguous mode
+  // is shorter; y row of index pp: (pp mod 2^pa_shift) * yst + (pp >> pa_shift) * ysb
+  int32_t pa_shift, ysb;
 };
 
 template <class A, int TY>
@@ -1024,7 +1029,9 @@ __global__ void __launch_bounds__(256) k_transpose_v4(const __grid_constant__ Tr
     for (int k = 0; k < SP; ++k) {
       const int32_t pp = it * PW + sr + SR * k;
       if (pp < a.et && qs < a.e0) {
-        T* yp = y + yb + pp * a.yst + qs;
+        const int32_t row = a.pa_shift ? (pp & ((1 << a.pa_shift) - 1)) * a.yst + (pp >> a.pa_shift) * a.ysb
+                                       : pp * a.yst;
+        T* yp = y + yb + row + qs;
         T o[4];
 #pragma unroll
         for (int i = 0; i < 4; ++i) o[i] = tile[sr + SR * k][sc4 + i];
@@ -1172,14 +1179,37 @@ static cudaError_t launch_perm_t(const PermArgs& a, int num_sms, cudaStream_t s)
                 a.ext[a.tmode] % 4 == 0 && (uintptr_t)a.x % 16 == 0 && (uintptr_t)a.y % 16 == 0 &&
                 a.xs[0] % 4 == 0 && a.ys[a.tmode] % 4 == 0;
       for (int m = 0; m < t.nb && v4; ++m) v4 = t.bxs[m] % 4 == 0 && t.bys[m] % 4 == 0;
+      t.pa_shift = 0;
+      t.ysb = 0;
       if constexpr (sizeof(T) == 4) {
         if (v4) {
-          const int pw = a.ext[a.tmode] <= 32 ? 32 : 64;   // tile width along x's contiguous mode
-          const int64_t tiles4 = ((a.ext[0] + 63) / 64) * ((a.ext[a.tmode] + pw - 1) / pw) *
-                                 (a.n / (a.ext[0] * a.ext[a.tmode]));
+          // x's contiguous mode of 8, 16 or 32 elements followed in x by a
+          // batch mode (x stride = its extent): tile over both, 256-byte x rows
+          const int64_t ec = a.ext[a.tmode];
+          int merge = -1;
+          if (ec >= 8 && ec <= 32 && (ec & (ec - 1)) == 0)
+            for (int m = 0; m < t.nb; ++m)
+              if (t.bxs[m] == ec && ec * (int64_t)t.bdiv[m].d >= 64 && t.bys[m] % 4 == 0) {
+                merge = m;
+                break;
+              }
+          if (merge >= 0) {
+            t.pa_shift = ec == 8 ? 3 : ec == 16 ? 4 : 5;
+            t.ysb = t.bys[merge];
+            t.et = (int32_t)(ec * t.bdiv[merge].d);
+            for (int m = merge; m + 1 < t.nb; ++m) {
+              t.bdiv[m] = t.bdiv[m + 1];
+              t.bxs[m] = t.bxs[m + 1];
+              t.bys[m] = t.bys[m + 1];
+            }
+            --t.nb;
+          }
+          const int64_t et = t.et;
+          const int pw = et <= 32 ? 32 : 64;   // tile width along x's contiguous run
+          const int64_t tiles4 = ((a.ext[0] + 63) / 64) * ((et + pw - 1) / pw) * (a.n / (a.ext[0] * et));
           t.ntiles = (uint32_t)tiles4;
           t.t0 = make_fastdiv((uint32_t)((a.ext[0] + 63) / 64));
-          t.tt = make_fastdiv((uint32_t)((a.ext[a.tmode] + pw - 1) / pw));
+          t.tt = make_fastdiv((uint32_t)((et + pw - 1) / pw));
           const int grid4 = (int)(tiles4 < maxgrid ? tiles4 : maxgrid);
           KernelTimer kt(s, "k_transpose_v4");
           if (pw == 32) k_transpose_v4<A, 32><<<grid4, 256, 0, s>>>(t);

@@ -494,3 +494,31 @@ def test_batch_innermost_tensor_core_gemm(code, sizes, prec, rtol):
         assert_match(to_np(yd), 3 * want + 2 * y0.astype(np.float64), "f32", rtol)
     finally:
         ome.set_einsum_backend(ome.B200Backend())
+
+
+@pytest.mark.parametrize("dt", ["f32", "trop"])
+@pytest.mark.parametrize("code,sizes", [
+    ("abcd->dcab", dict(a=8, b=9, c=12, d=64)),      # x's contiguous mode of 8 merged with b: 72-wide rows
+    ("abcd->dcab", dict(a=16, b=5, c=7, d=36)),
+    ("abcd->dcab", dict(a=16, b=3, c=7, d=36)),      # 48 < 64: not merged
+    ("abcd->dcab", dict(a=32, b=6, c=2, d=128)),
+    ("abcde->ecadb", dict(a=32, b=32, c=4, d=4, e=128)),   # the rule-suite permutation, smaller
+])
+def test_transpose_merged_x_rows(dt, code, sizes):
+    """k_transpose_v4 (Float32) with x's short contiguous mode and the next x
+    mode tiled together (256-byte x rows): exact against the oracle, with and
+    without alpha-beta; the same permutations of tropical numbers."""
+    rng = np.random.default_rng(zlib.crc32(code.encode()) + sizes["a"])
+    ixs, iy = parse(code)
+    x = gen(rng, [sizes[l] for l in ixs[0]], dt)
+    y0 = gen(rng, [sizes[l] for l in iy], dt)
+    for sx, sy in [(True, False)] + ([(2.0, 0.5)] if dt == "f32" else []):
+        yd = to_dev(y0, dt)
+        ynp = to_np(yd).copy()
+        out, names = kernel_names(lambda: ome.einsum_(ome.ein(code), [to_dev(x, dt)], yd, sx, sy, sizes))
+        want = oracle(ixs, iy, [x], sizes, dt)
+        if not (sx is True and sy is False):
+            want = sx * want + sy * ynp
+        if dt == "f32":   # (tropical numbers here are 8 bytes: k_transpose32)
+            assert "k_transpose_v4" in names, names
+        assert_match(to_np(yd), want, dt)
