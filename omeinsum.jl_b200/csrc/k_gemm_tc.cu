@@ -1242,11 +1242,14 @@ template <int NT>
 __device__ __forceinline__ void split8_store(float (&v)[8], uint32_t dst) {
 #pragma unroll
   for (int t = 0; t < NT; ++t) {
+    // the third term of a 3-term split is truncated: its error (below 2^-24
+    // of the value) is under that of the products the split leaves out
+    const uint32_t half = NT == 3 && t == 2 ? 0u : 0x8000u;
     uint32_t w[4];
 #pragma unroll
     for (int p = 0; p < 4; ++p) {
-      const uint32_t ra = __float_as_uint(v[2 * p]) + 0x8000u;
-      const uint32_t rb = __float_as_uint(v[2 * p + 1]) + 0x8000u;
+      const uint32_t ra = __float_as_uint(v[2 * p]) + half;
+      const uint32_t rb = __float_as_uint(v[2 * p + 1]) + half;
       w[p] = __byte_perm(ra, rb, 0x7632);   // (ra >> 16) | (rb & 0xffff0000)
       if (t + 1 < NT) {
         v[2 * p] -= __uint_as_float(ra & 0xffff0000u);
@@ -2328,7 +2331,7 @@ template <int NT>
 __device__ __forceinline__ void split_terms(float x, uint32_t (&t)[NT]) {
 #pragma unroll
   for (int u = 0; u < NT; ++u) {
-    const uint32_t r = __float_as_uint(x) + 0x8000u;
+    const uint32_t r = __float_as_uint(x) + (NT == 3 && u == 2 ? 0u : 0x8000u);   // last of 3: truncated
     t[u] = r;
     if (u + 1 < NT) x -= __uint_as_float(r & 0xffff0000u);
   }
