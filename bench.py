@@ -344,7 +344,36 @@ def tn_section(ome, dev, n=180, sc_target=27):
     out["bf16x3"]["frac_of_bf16x3_peak"] = out["bf16x3"]["tflops"] / (bf16 / 3)
     out["speedup_bf16x6_vs_fp32"] = out["fp32"]["s"] / out["bf16x6"]["s"]
     ome.set_einsum_backend(ome.B200Backend())
+    out["_cpu_job"] = (se, sd, xs)   # for the CPU leg (popped before printing)
     return out
+
+
+def _oracle_tree(O, ne):
+    """The package's NestedEinsum as the oracle's tree."""
+    if ne.isleaf:
+        return O.leaf(ne.tensorindex)
+    return O.Node(args=[_oracle_tree(O, a) for a in ne.args], ixs=[list(ix) for ix in ne.eins.ixs],
+                  iy=list(ne.eins.iy))
+
+
+def tn_cpu_baseline(O, job, nsample=1):
+    """The oracle's sliced evaluation of the n = 180 network on the host cores,
+    FP32 and FP64, over the first nsample slices; the whole contraction's time
+    is that times nslices / nsample (slices have equal shapes)."""
+    se, sd, xs = job
+    tree = _oracle_tree(O, se.eins)
+    nsl = 2 ** len(se.slicing)
+    res = {}
+    for name, dt in (("fp32", np.float32), ("fp64", np.float64)):
+        xd = [np.asfortranarray(x.astype(dt)) for x in xs]
+        t0 = time.perf_counter()
+        O.sliced_partial(list(se.slicing), tree, xd, sd, 0, nsample)
+        t = time.perf_counter() - t0
+        res[name] = {"s_per_contraction": t * nsl / nsample, "contractions_per_s": nsample / (t * nsl)}
+    res.update({"cores": os.cpu_count(), "kind": "port",
+                "sample": f"{nsample} of {nsl} slices, oracle (NumPy/OpenBLAS) tree evaluation, scaled by "
+                          f"{nsl}/{nsample}"})
+    return res
 
 
 def tn_sharded_section(ome, dev, world, n=180, sc_target=27):
@@ -863,6 +892,10 @@ def main():
     ome.release_workspaces()
     torch.cuda.empty_cache()
     tn = None if (args.no_tn or world > 1) else tn_section(ome, dev)
+    if tn is not None:
+        job = tn.pop("_cpu_job")
+        if cpu is not None:   # the CPU leg ran: the oracle on a sample of the slices
+            tn["cpu_baseline"] = tn_cpu_baseline(O, job)
     ome.release_workspaces()
     torch.cuda.empty_cache()
     sharded = tn_sharded_section(ome, dev, world) if (grouped and not args.no_tn) else None
@@ -880,6 +913,17 @@ def main():
                 batch[key]["rel_err_vs_oracle"] = {"jobs": len(smp), "max": max(errs[cfg]),
                                                    "median": float(np.median(errs[cfg])),
                                                    "reference": "oracle (ComplexF64 NumPy restatement)"}
+            # CPU baseline: the sampled jobs as a NumPy ComplexF32 loop (tensordot = BLAS CGEMM)
+            reps = 3
+            t0 = time.perf_counter()
+            for _ in range(reps):
+                for j, xs, _, _ in smp:
+                    t = np.tensordot(xs[0], xs[1], axes=(1, 0))      # (a, c, d)
+                    np.tensordot(t, xs[2], axes=(2, 0))             # (a, c, e)
+            tc = (time.perf_counter() - t0) / reps
+            batch["cpu_baseline"] = {"jobs_per_s": len(smp) / tc, "unit": "jobs/s", "cores": os.cpu_count(),
+                                     "kind": "port", "sample": f"{len(smp)} of the jobs, {reps} passes, NumPy "
+                                                               "complex64 tensordot loop"}
     serve = None if (args.no_serve or world > 1) else serve_section(ome, dev)
     detail = {}
     for (nm, code, ext, _), ms in zip(CASES, per_case):
