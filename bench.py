@@ -583,7 +583,7 @@ def serve_section(ome, dev, njobs=400, rate=2000.0, seed=10, nmin=40, nmax=200, 
     # relative error of the served values against FP64 on the same trees
     ome.release_workspaces()
     torch.cuda.empty_cache()
-    errs, t_ref = [], time.perf_counter()
+    errs, refs, t_ref = [], {}, time.perf_counter()
     order = sorted(done, key=lambda j: raw[pos[id(j)]][4])
     for j in order:
         if time.perf_counter() - t_ref > ref_cap_s:
@@ -593,6 +593,7 @@ def serve_section(ome, dev, njobs=400, rate=2000.0, seed=10, nmin=40, nmax=200, 
         ref = float(ref.double().cpu()) * 2.0 ** lg
         if ref != 0 and math.isfinite(ref):
             errs.append(abs(j.scalar() - ref) / abs(ref))
+            refs[pos[id(j)]] = ref
     # the same stream through the library's own serving loop (ome_server_*):
     # admission, slots and issue threads in C++, the same rules
     ome.release_workspaces()
@@ -610,8 +611,11 @@ def serve_section(ome, dev, njobs=400, rate=2000.0, seed=10, nmin=40, nmax=200, 
     same = sum(1 for a, b in both if torch.equal(a.value, b.value))
     # kernels may differ between the two runs where a GEMM's operand buffer
     # depends on free device memory, so values agree to rounding, not always bitwise
-    vdiff = max((float((a.value.double() - b.value.double()).abs().max() / b.value.double().abs().max())
+    vdiff = max((float((a.value.double() - b.value.double()).abs().max()
+                       / max(a.value.double().abs().max(), b.value.double().abs().max()))
                  for a, b in both if float(b.value.double().abs().max()) > 0), default=0.0)
+    nerrs = [abs(b.scalar() - refs[i]) / abs(refs[i]) for i, b in enumerate(njobs_native)
+             if i in refs and id(b) in ndone]
     nlat = np.array([j.done - j.arrival for j in nsrv.finished]) if nsrv.finished else np.zeros(1)
     reasons = [j.reject_reason for j in nsrv.rejected]   # this stream only (the library counts both passes)
     native = {"completed": len(nsrv.finished), "rejected_over_work_cap": reasons.count("work"),
@@ -627,6 +631,10 @@ def serve_section(ome, dev, njobs=400, rate=2000.0, seed=10, nmin=40, nmax=200, 
               if nsrv.finished else 0.0,
               "values_identical_to_python_server": f"{same}/{len(both)}",
               "max_rel_diff_vs_python_server": vdiff,
+              "rel_err_vs_fp64": {"jobs": len(nerrs), "max": max(nerrs) if nerrs else None,
+                                  "median": float(np.median(nerrs)) if nerrs else None,
+                                  "within_1e-5": sum(e <= 1e-5 for e in nerrs),
+                                  "reference": "the same FP64 values as the Python server's check"},
               "api": "ome_server_create/submit/poll/stats (C ABI), driven by NativeTNServer"}
     lat = np.array([j.latency for j in done]) if done else np.zeros(1)
     st.update({"workload": f"{njobs} jobs, Poisson {rate:.0f}/s (seed {seed}), n uniform even [{nmin},{nmax}], "

@@ -353,8 +353,10 @@ OME_API int ome_server_create(int device, int32_t n_slots, size_t hbm_budget_byt
  * (dxs[t] receives the gradient of input t; the plan runs unsliced).  inputs,
  * y and dxs are column-major contiguous device buffers of the plan's dtype;
  * they and the plan belong to the caller and must stay valid until poll
- * reports the job.  input_stream (may be NULL): the stream the inputs were
- * written on; the job's kernels wait for that stream's work at submit time.
+ * reports the job.  input_stream: the stream the inputs were written on (NULL
+ * = the legacy default stream, as in every CUDA call); the job's kernels run
+ * after the work queued on it at submit time -- the slots' streams are
+ * non-blocking and would not otherwise wait for the default stream.
  * work: the job's multiply-adds, for the work cap.  Thread-safe with poll. */
 OME_API int ome_server_submit(ome_server* server, ome_plan* plan, int32_t ninputs, const void* const* inputs,
                               void* y, void* const* dxs, double work, void* input_stream, int64_t* job_id);

@@ -43,7 +43,7 @@ struct SrvJob {
   void* y = nullptr;
   std::vector<void*> dxs;        // empty: a value job
   double work = 0;               // multiply-adds (for the work cap)
-  cudaEvent_t ready = nullptr;   // inputs ready: recorded on the caller's stream at submit
+  cudaEvent_t ready = nullptr;   // the caller's stream at submit (inputs and outputs ready)
   cudaEvent_t done_ev = nullptr;
   double arrival = 0, admitted = -1, done = -1;
   int status = OME_OK;
@@ -325,10 +325,11 @@ int ome_server_submit(ome_server* s, ome_plan* plan, int32_t ninputs, const void
   if (dxs) j->dxs.assign(dxs, dxs + ninputs);
   j->work = work;
   cudaError_t e = cudaEventCreateWithFlags(&j->done_ev, cudaEventDisableTiming);
-  if (e == cudaSuccess && input_stream) {
-    e = cudaEventCreateWithFlags(&j->ready, cudaEventDisableTiming);
-    if (e == cudaSuccess) e = cudaEventRecord(j->ready, static_cast<cudaStream_t>(input_stream));
-  }
+  // the job's kernels run after the work already queued on input_stream (NULL
+  // is the legacy default stream, as everywhere in CUDA): the slots' streams
+  // are non-blocking, so without this event they would not wait for it
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&j->ready, cudaEventDisableTiming);
+  if (e == cudaSuccess) e = cudaEventRecord(j->ready, static_cast<cudaStream_t>(input_stream));
   if (e != cudaSuccess) {
     free_job(j);
     return cuda_err(e, "job events");

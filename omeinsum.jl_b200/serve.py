@@ -385,8 +385,10 @@ class NativeTNServer:
         self._t0 = None            # server clock at the start of run_trace (None: report the library's times)
 
     def submit(self, job: Job) -> int:
-        """Plan the job, allocate its outputs and queue it; inputs written on
-        the current stream are waited for by the job's kernels."""
+        """Plan the job, allocate its outputs and queue it; the job's kernels
+        run after the work queued on the current stream (the legacy default
+        stream too: its handle 0 is passed as NULL, which the library reads as
+        that stream)."""
         p = _Prepared(job.xs)
         ts = [_f_contig(t) for t in p.tensors]
         sd = get_size_dict(job.code.getixsv(), ts)

@@ -113,3 +113,26 @@ def test_batch_graph_replays_the_grouped_launches(tile_config):
     torch.cuda.synchronize()
     for y, ye in zip(b2.outputs, eager):
         assert torch.allclose(y, 2 * ye, rtol=1e-6, atol=0)
+
+
+def test_native_server_waits_for_the_submitting_stream():
+    """Inputs written on the default stream just before submit (behind a long
+    fill): the jobs' kernels on the slots' non-blocking streams must run after
+    them.  Values against the oracle."""
+    nets = [network(24 + 4 * i, 300 + i) for i in range(8)]
+    big = torch.empty(1 << 28, device="cuda")   # 1 GiB: a fill of ~0.2 ms on the default stream
+    srv = ome.NativeTNServer(n_slots=8, hbm_budget_bytes=8e9)
+    jobs = []
+    for i, (o, sd, xs) in enumerate(nets):
+        big.fill_(float(i))
+        ys = [x * 1.0 for x in xs]              # queued behind the fill
+        jobs.append(ome.Job(o, ys))
+        srv.submit(jobs[-1])
+        srv.poll()
+    while srv.poll() or srv._live:
+        pass
+    srv.close()
+    assert len(srv.finished) == len(nets)
+    for job, (o, sd, xs) in zip(jobs, nets):
+        want = O.nested_einsum(_tree(o), [x.double().cpu().numpy() for x in xs], sd)
+        assert abs(job.scalar() - float(want)) <= 1e-5 * abs(float(want))
